@@ -1,0 +1,340 @@
+"""Benchmark of the sm_100a GF(2^16) erasure-coding path.
+
+Default workload (one GPU): the large-encode configuration -- 4 files x
+512 MiB of seeded uniform random bytes, 1 MiB slices -> k = 2048 source
+slices, r = 205 recovery slices (10 %), recovery data computed by the region
+multiply-accumulate.  One "step" is one full encode of that set.
+
+  value   source GB/s with the slices resident in HBM (device pointers through
+          the C ABI, CUDA events on the launching stream, max over ranks)
+  e2e     the same through the C ABI with pinned HOST buffers: the 2 GiB H2D
+          copy of the sources and the D2H copy of the 205 recovery slices are
+          inside the timed region
+  roofline  the multiply-accumulate kernel's integer-issue roofline: 2 LOP3
+          per symbol multiply-accumulate against the LOP3 rate measured on
+          this device, plus its HBM side
+  cpu_baseline  the reference's CPU strategy (par2-rs AVX2-Shuffle restated
+          in C, all host threads) on a bounded column sample of the same set
+
+``--impl reference`` times that CPU strategy alone (rank 0) and prints the
+reference line.  Multi-GPU (torchrun): every rank encodes its own set
+(independent recovery sets, weak scaling, no data-path collective).
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "par2-rs_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] \
+    if os.path.exists(os.path.join(ROOT, "BASELINE.json")) else "encode GB/s"
+K_SRC, SLICE, R_REC = 2048, 1 << 20, 205
+WORKLOAD = "large_encode: 4 files x 512 MiB seeded uniform random, 1 MiB slices, k=2048, r=205 (10%)"
+SEED = 20261203
+CPU_SAMPLE_BYTES = 48 * 1024  # columns of every slice in the CPU sample
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def probe_int_peak(device):
+    lib = ctypes.CDLL(os.path.join(ROOT, "par2-rs_b200", "lib", "libp2g_probe.so"))
+    ops = ctypes.c_double()
+    ms = ctypes.c_double()
+    sms = ctypes.c_int()
+    rc = lib.p2g_probe_lop3(device, ctypes.byref(ops), ctypes.byref(ms), ctypes.byref(sms))
+    if rc != 0:
+        return None, None
+    return ops.value, sms.value
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gen_sources(k, S, seed):
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 256, (k, S), dtype=np.uint8)
+
+
+def cpu_encode_rate(src_host, k, S, r, threads):
+    """The restated par2-rs AVX2 strategy on a column sample of every slice:
+    returns (source GB/s, seconds, sample bytes, recovery sample)."""
+    from oracle import oracle
+
+    sample = np.ascontiguousarray(src_host[:, :CPU_SAMPLE_BYTES])
+    t0 = time.perf_counter()
+    rec = oracle.cpu_encode(sample, r, threads)
+    dt = time.perf_counter() - t0
+    return sample.nbytes / dt / 1e9, dt, sample.nbytes, rec
+
+
+def traffic_from_profile():
+    path = os.path.join(ROOT, "profiles", "muladd_large_encode_traffic.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path)).get("dram_bytes_per_launch")
+        except ValueError:
+            return None
+    return None
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    k, S, r = K_SRC, SLICE, R_REC
+    threads = os.cpu_count() or 1
+    src = gen_sources(k, CPU_SAMPLE_BYTES, SEED)
+    from oracle import oracle
+
+    for _ in range(args.warmup):
+        oracle.cpu_encode(src, r, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.cpu_encode(src, r, threads)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times) / len(times)
+    gbs = src.nbytes / dt / 1e9
+    sample = f"all {k} slices x first {CPU_SAMPLE_BYTES // 1024} KiB columns, r={r}, per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u16 (GF(2^16))", "data": "synthetic (seeded uniform bytes)",
+        "config": {"workload": WORKLOAD, "sample": sample},
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": sample,
+                         "what": "par2-rs AVX2-Shuffle strategy restated in C (Rust reference "
+                                 "not buildable here), reference threading"},
+        "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+
+    import par2gpu
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    k, S, r = K_SRC, SLICE, R_REC
+    exps = np.arange(r, dtype=np.uint32)
+
+    src_host_np = gen_sources(k, S, SEED + rank)
+    src_pinned = torch.from_numpy(src_host_np).pin_memory()
+    out_pinned = torch.zeros((r, S), dtype=torch.uint8).pin_memory()
+    src_dev = src_pinned.to(dev)
+    out_dev = torch.zeros((r, S), dtype=torch.uint8, device=dev)
+
+    ctx = par2gpu.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    src_ptrs = [src_dev[i] for i in range(k)]
+    out_ptrs = [out_dev[e] for e in range(r)]
+
+    def step_dev():
+        ctx.encode(src_ptrs, S, exps, out_ptrs, device=True)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world > 1:
+            t = torch.tensor([v], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return v
+
+    # ---- device-resident timed region (value) ----
+    for _ in range(args.warmup):
+        step_dev()
+    ctx.set_timing(True)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    mul_ms, launches = [], 0
+    for _ in range(args.steps):
+        step_dev()
+        t = ctx.last_timing()
+        mul_ms.append(t.ms_muladd)
+        launches += t.launches
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier()
+    ms_step = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    ctx.set_timing(False)
+    value = world * k * S / (ms_step * 1e-3) / 1e9
+
+    # ---- end to end through the C ABI with pinned host buffers (e2e) ----
+    src_h = src_pinned.numpy()
+    out_h = out_pinned.numpy()
+    host_src = [src_h[i] for i in range(k)]
+    host_out = [out_h[e] for e in range(r)]
+    e2e_steps = max(1, args.steps)
+    ctx.encode(host_src, S, exps, host_out)  # warm the staging buffers
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        ctx.encode(host_src, S, exps, host_out)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+    e2e_value = world * k * S / (e2e_ms * 1e-3) / 1e9
+
+    # ---- roofline of the multiply-accumulate kernel ----
+    int_peak, sms = probe_int_peak(local)
+    hbm_peak, peak_kind = peaks()
+    t_kernel = sum(mul_ms) / len(mul_ms) * 1e-3
+    macs = k * r * (S // 2)
+    int_ops = 2.0 * macs
+    alg_bytes = (k + r) * S
+    roofline = {
+        "bound": "int",
+        "kernel": "muladd_bitsliced",
+        "achieved": int_ops / t_kernel / 1e12,
+        "peak": (int_peak or 0) / 1e12,
+        "unit": "Tops/s (2 LOP3 per GF(2^16) symbol MAC)",
+        "frac": (int_ops / t_kernel) / int_peak if int_peak else None,
+        "peak_source": f"LOP3 issue rate measured on this device ({sms} SMs)",
+        "kernel_ms": t_kernel * 1e3,
+        "alg_bytes": alg_bytes,
+        "hbm": {"achieved": alg_bytes / t_kernel / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": alg_bytes / t_kernel / 1e9 / hbm_peak, "peak_source": peak_kind},
+        "traffic": traffic_from_profile(),
+    }
+
+    # ---- CPU baseline + bit-exact cross-check on the same column sample ----
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        gbs, dt, nbytes, rec_sample = cpu_encode_rate(src_host_np, k, S, r, threads)
+        dev_sample = out_dev[:, :CPU_SAMPLE_BYTES].cpu().numpy()
+        cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"all {k} slices x first {CPU_SAMPLE_BYTES // 1024} KiB columns, r={r}",
+               "seconds": dt,
+               "what": "par2-rs AVX2-Shuffle strategy restated in C, reference threading",
+               "gpu_matches_sample": bool(np.array_equal(dev_sample, rec_sample))}
+    ctx.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u16 (GF(2^16))", "data": "synthetic (seeded uniform bytes)",
+            "config": {"workload": WORKLOAD, "k": k, "r": r, "slice_bytes": S,
+                       "parallelism": f"{world} independent sets" if world > 1 else "1 set",
+                       "l2": "inputs 2 GiB per step > 126 MB L2; no flush"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "GB/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": k * S, "d2h_bytes_per_step": r * S},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

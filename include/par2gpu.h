@@ -1,0 +1,148 @@
+/*
+ * par2gpu.h -- C ABI of the B200 (sm_100a) GF(2^16) erasure-coding library.
+ *
+ * The entry points are what a par2-rs backend binds through FFI.  Each one
+ * names the par2-rs interface it stands in for (paths are relative to the
+ * par2-rs repository root).  All symbols are plain C: pointers, sizes and
+ * integer status codes, no C++ or torch types.
+ *
+ * Conventions
+ *   - Slices are byte arrays; a GF(2^16) symbol is a little-endian u16
+ *     (par2-rs galois/mod.rs:178-223).  Slice lengths in bytes must be even.
+ *   - Every call returns P2G_OK (0) or a negative P2G_E* code; the message of
+ *     the last failure on the calling thread is p2g_last_error().
+ *   - Pointers are host pointers unless P2G_DEVICE_PTRS is passed, in which
+ *     case every slice pointer (not the pointer arrays themselves, which are
+ *     always host arrays) is a device pointer on the context's device.
+ *   - The caller owns all buffers.  A context serialises its calls with an
+ *     internal lock, so one context may be shared by threads (as par2-rs
+ *     shares its Send + Sync strategy object, galois/simd/mod.rs:24); for
+ *     concurrency give each thread its own context.
+ */
+#ifndef PAR2GPU_H
+#define PAR2GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define P2G_OK 0
+#define P2G_EINVAL (-1)     /* bad argument (odd length, null pointer, k = 0 ...) */
+#define P2G_ENOMEM (-2)     /* device or pinned allocation failed */
+#define P2G_ECUDA (-3)      /* a CUDA runtime call failed */
+#define P2G_ESINGULAR (-4)  /* "Singular matrix" (par2_rs.rs:361-370) */
+#define P2G_ETIMEOUT (-5)   /* a bounded device wait gave up */
+#define P2G_ENODEV (-6)     /* no usable sm_100 device */
+#define P2G_ERANGE (-7)     /* a size beyond a documented maximum */
+
+/* flags */
+#define P2G_DEVICE_PTRS 0x1u /* slice pointers are device pointers */
+
+/* strategy priority values, par2-rs galois/simd/mod.rs:14-21 */
+#define P2G_PRIORITY_FALLBACK 0
+#define P2G_PRIORITY_BASIC 10
+#define P2G_PRIORITY_ENHANCED 20
+#define P2G_PRIORITY_ADVANCED 30
+#define P2G_PRIORITY_OPTIMAL 40
+
+typedef struct p2g_ctx p2g_ctx;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *p2g_last_error(void);
+
+/* Library / device context.  Replaces the lazily initialised global state of
+ * par2-rs (galois/core.rs:49-91 tables, galois/simd/mod.rs:237-242 registry)
+ * with an explicit handle bound to one CUDA device. */
+int p2g_create(int device, p2g_ctx **out);
+int p2g_destroy(p2g_ctx *ctx);
+
+/* Runs the context's work on a caller-supplied CUDA stream (a cudaStream_t
+ * passed as void*; NULL restores the context's own stream).  Calls still
+ * return only when their work is complete.  No counterpart in par2-rs: it is
+ * the device-side plumbing a host integration needs. */
+int p2g_set_stream(p2g_ctx *ctx, void *cuda_stream);
+
+/* Per-phase device times of the last call, measured with CUDA events on the
+ * stream the kernels run on when timing is enabled.  No counterpart in
+ * par2-rs (its tracing is host-side, par2_rs.rs:220-226). */
+typedef struct {
+    float ms_records;  /* coefficient records */
+    float ms_planes;   /* slices -> bit planes */
+    float ms_muladd;   /* the multiply-accumulate kernel */
+    float ms_total;    /* first to last event of the call */
+    int launches;      /* kernels launched by the call */
+} p2g_timing;
+int p2g_set_timing(p2g_ctx *ctx, int enable);
+int p2g_last_timing(p2g_ctx *ctx, p2g_timing *out);
+
+/* GaloisSimdStrategy::{name, is_available, priority}
+ * (galois/simd/mod.rs:26-33): "CUDA-sm100a", available iff an sm_100 device
+ * is present, priority P2G_PRIORITY_OPTIMAL. */
+int p2g_strategy_info(const char **name, int *priority, int *available);
+
+/* GaloisSimdStrategy::mul_slice (galois/simd/mod.rs:39): data[i] = c * data[i]
+ * over n u16 symbols. */
+int p2g_mul_slice(p2g_ctx *ctx, uint16_t c, uint16_t *data, size_t n, uint32_t flags);
+
+/* GaloisSimdStrategy::muladd (galois/simd/mod.rs:45):
+ * dst[i] ^= c * src[i] over n u16 symbols. */
+int p2g_muladd(p2g_ctx *ctx, uint16_t *dst, const uint16_t *src, size_t n, uint16_t c,
+               uint32_t flags);
+
+/* GaloisSimdStrategy::muladd_region (galois/simd/mod.rs:51-58), also the
+ * target of gf_muladd_block_regions (galois/region/mod.rs:195-242):
+ *   dsts[d][off .. off+len) ^= sum_s coeff_rows[d][s] * srcs[s][off .. off+len)
+ * with coeff_rows[d] an array of nsrc coefficients (coefficients[dst][src]),
+ * off and len in u16 units. */
+int p2g_muladd_region(p2g_ctx *ctx, uint16_t *const *dsts, size_t ndst,
+                      const uint16_t *const *srcs, size_t nsrc,
+                      const uint16_t *const *coeff_rows, size_t off_u16, size_t len_u16,
+                      uint32_t flags);
+
+/* PAR2 input-slice constants (par2_rs.rs:64-76 generate_par2_constants):
+ * out[i] = 2^n_i, n_i the i-th n >= 1 not divisible by 3, 5, 17 or 257. */
+int p2g_par2_constants(size_t k, uint16_t *out);
+
+/* Recovery-slice creation, the work of Par2ReedSolomon::create_streaming_encoder
+ * + StreamingEncoder::{process_block, flush_batch, finalize}
+ * (par2_rs.rs:687-902): out[e] = sum_i c_i^{exps[e]} * src[i] for k input
+ * slices of slice_bytes (the caller zero-pads the last slice of a file, as
+ * creator.rs:386-395 does).  out receives r recovery slice bodies. */
+int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_bytes,
+               const uint32_t *exps, size_t r, uint8_t *const *out, uint32_t flags);
+
+/* Exact GF(2^16) inverse of an m x m matrix (row-major host arrays), by
+ * Gauss-Jordan on the device -- the elimination par2-rs performs in
+ * Par2ReedSolomon::compute_reconstruction_transform (par2_rs.rs:355-401).
+ * Returns P2G_ESINGULAR ("Singular matrix", :361-370) when A has no inverse. */
+int p2g_invert(p2g_ctx *ctx, size_t m, const uint16_t *A, uint16_t *inv);
+
+/* The repair decode matrix A^-1 (m x m, row-major) for
+ * A[row][col] = c_{missing[col]}^{exps[row]}, c_i the PAR2 constants of k
+ * input slices (par2_rs.rs:346-353). */
+int p2g_reconstruction_matrix(p2g_ctx *ctx, size_t k, const uint64_t *missing, size_t m,
+                              const uint32_t *exps, uint16_t *inv);
+
+/* Repair: Par2ReedSolomon::compute_reconstruction_transform +
+ * reconstruct_streaming_chunk over whole slices (par2_rs.rs:319-675).
+ *   k           input slices in the set (fixes the constants c_i)
+ *   missing[m]  strictly ascending global indices of the slices to rebuild
+ *   present     the k - m other input slices, ascending index order
+ *   exps[m], recovery[m]  the recovery slices used; par2-rs takes the m
+ *               lowest exponents (repair.rs:585-604)
+ *   out[m]      out[j] receives slice missing[j]
+ * Computes out = A^-1 (R ^ V * present) with V[row][j] = c_{present_j}^{exps[row]}.
+ * Returns P2G_ESINGULAR when A is singular. */
+int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missing, size_t m,
+               const uint8_t *const *present, const uint32_t *exps,
+               const uint8_t *const *recovery, uint8_t *const *out, uint32_t flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PAR2GPU_H */

@@ -1,0 +1,715 @@
+// capi.cu -- the C ABI of libpar2gpu (include/par2gpu.h): contexts, staging
+// of host / misaligned buffers, argument checking and error reporting.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "invert.cuh"
+#include "muladd.cuh"
+
+namespace p2g {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+int DevBuf::ensure(size_t n)
+{
+    if (n <= cap)
+        return P2G_OK;
+    release();
+    size_t want = n < 4096 ? 4096 : n;
+    cudaError_t e = pinned ? cudaMallocHost(&p, want) : cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cap = 0;
+        (void)cudaGetLastError();
+        set_error("%s of %zu bytes failed: %s", pinned ? "cudaMallocHost" : "cudaMalloc", want,
+                  cudaGetErrorString(e));
+        return P2G_ENOMEM;
+    }
+    cap = want;
+    return P2G_OK;
+}
+
+void DevBuf::release()
+{
+    if (p) {
+        if (pinned)
+            cudaFreeHost(p);
+        else
+            cudaFree(p);
+    }
+    p = nullptr;
+    cap = 0;
+}
+
+static size_t round16(size_t n) { return (n + 15) & ~static_cast<size_t>(15); }
+
+// PAR2 constants (par2_rs.rs:64-76), with the GF tables of galois/core.rs:49-91.
+struct HostTables {
+    uint16_t log[65536];
+    uint16_t exp[65535];
+    HostTables()
+    {
+        uint32_t b = 1;
+        for (uint32_t l = 0; l < 65535; ++l) {
+            exp[l] = static_cast<uint16_t>(b);
+            log[b] = static_cast<uint16_t>(l);
+            b <<= 1;
+            if (b & 0x10000u)
+                b ^= 0x1100Bu;
+        }
+        log[0] = 0;
+    }
+};
+
+static const HostTables &tables()
+{
+    static HostTables t;
+    return t;
+}
+
+static void par2_constants(size_t k, uint16_t *out)
+{
+    const HostTables &t = tables();
+    size_t have = 0;
+    for (uint64_t n = 1; have < k; ++n)
+        if (n % 3 && n % 5 && n % 17 && n % 257)
+            out[have++] = t.exp[n % 65535];
+}
+
+// Layout of the per-call parameter block (device + pinned mirror).
+struct ParamLayout {
+    size_t src_off, dst_off, a_off, b_off, total;
+    ParamLayout(size_t nsrc, size_t ndst, size_t a_bytes, size_t b_bytes)
+    {
+        src_off = 0;
+        dst_off = round16(nsrc * sizeof(void *));
+        a_off = dst_off + round16(ndst * sizeof(void *));
+        b_off = a_off + round16(a_bytes);
+        total = b_off + round16(b_bytes);
+    }
+};
+
+static int upload_params(p2g_ctx *ctx, const ParamLayout &L)
+{
+    P2G_CUDA(cudaMemcpyAsync(ctx->params.p, ctx->hparams.p, L.total, cudaMemcpyHostToDevice,
+                             ctx->stream));
+    return P2G_OK;
+}
+
+static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Resolves the slice pointers a kernel will use: device pointers that are
+// 16-byte aligned are used in place; host pointers (or misaligned device
+// pointers) are staged through `buf` (one padded slot per slice).  `copy_in`
+// copies the current contents in.
+static int stage(p2g_ctx *ctx, p2g::DevBuf &buf, const uint8_t *const *ptrs, size_t n,
+                 size_t bytes, bool device, bool copy_in, std::vector<uint8_t *> &out,
+                 bool &staged)
+{
+    out.resize(n);
+    bool all_ok = device;
+    if (device)
+        for (size_t i = 0; i < n; ++i)
+            if (!aligned16(ptrs[i]))
+                all_ok = false;
+    staged = !all_ok;
+    if (all_ok) {
+        for (size_t i = 0; i < n; ++i)
+            out[i] = const_cast<uint8_t *>(ptrs[i]);
+        return P2G_OK;
+    }
+    size_t slot = round16(bytes);
+    P2G_TRY(buf.ensure(slot * (n ? n : 1)));
+    for (size_t i = 0; i < n; ++i) {
+        out[i] = buf.as<uint8_t>() + i * slot;
+        if (copy_in)
+            P2G_CUDA(cudaMemcpyAsync(out[i], ptrs[i], bytes,
+                                     device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    }
+    return P2G_OK;
+}
+
+static int unstage(p2g_ctx *ctx, uint8_t *const *user, const std::vector<uint8_t *> &dev,
+                   size_t n, size_t bytes, bool device)
+{
+    for (size_t i = 0; i < n; ++i)
+        P2G_CUDA(cudaMemcpyAsync(user[i], dev[i], bytes,
+                                 device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    return P2G_OK;
+}
+
+// Starts a call: resets the launch counter and the timing marks.
+static void begin(p2g_ctx *ctx)
+{
+    ctx->launches = 0;
+    for (bool &m : ctx->ev_marked)
+        m = false;
+    ctx->mark(0);
+}
+
+static float elapsed(p2g_ctx *ctx, int a, int b)
+{
+    float ms = 0.f;
+    if (ctx->ev_marked[a] && ctx->ev_marked[b] &&
+        cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]) != cudaSuccess) {
+        (void)cudaGetLastError();
+        ms = 0.f;
+    }
+    return ms;
+}
+
+// Ends a call: waits for its work and collects the timing.
+static int finish(p2g_ctx *ctx)
+{
+    ctx->mark(4);
+    P2G_CUDA(cudaStreamSynchronize(ctx->stream));
+    P2G_CUDA(cudaGetLastError());
+    ctx->last = p2g_timing{};
+    ctx->last.launches = ctx->launches;
+    if (ctx->timing) {
+        ctx->last.ms_records = elapsed(ctx, 0, 1);
+        ctx->last.ms_planes = elapsed(ctx, 1, 2);
+        ctx->last.ms_muladd = elapsed(ctx, 2, 3);
+        ctx->last.ms_total = elapsed(ctx, 0, 4);
+    }
+    return P2G_OK;
+}
+
+// Generic coefficient-matrix muladd over resolved device slices:
+// dst[o] (^)= sum_i coeff[o][i] * src[i]; coeff is a host [nout][nin] matrix.
+static int matrix_muladd(p2g_ctx *ctx, const std::vector<uint8_t *> &src,
+                         const std::vector<uint8_t *> &dst, const uint16_t *coeff,
+                         size_t bytes, int mode)
+{
+    size_t nin = src.size(), nout = dst.size();
+    ParamLayout L(nin, nout, nin * nout * 2, 0);
+    P2G_TRY(ctx->hparams.ensure(L.total));
+    P2G_TRY(ctx->params.ensure(L.total));
+    uint8_t *h = ctx->hparams.as<uint8_t>();
+    memcpy(h + L.src_off, src.data(), nin * sizeof(void *));
+    memcpy(h + L.dst_off, dst.data(), nout * sizeof(void *));
+    memcpy(h + L.a_off, coeff, nin * nout * 2);
+    P2G_TRY(upload_params(ctx, L));
+    uint8_t *d = ctx->params.as<uint8_t>();
+    P2G_TRY(ctx->recs.ensure(nin * nout * 64));
+    P2G_TRY(records_from_matrix(ctx, reinterpret_cast<const uint16_t *>(d + L.a_off),
+                                static_cast<int>(nin), static_cast<int>(nout),
+                                ctx->recs.as<uint32_t>()));
+    P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(d + L.src_off),
+                       static_cast<int>(nin), reinterpret_cast<uint8_t *const *>(d + L.dst_off),
+                       static_cast<int>(nout), bytes, ctx->recs.as<uint32_t>(), mode));
+    return P2G_OK;
+}
+
+}  // namespace p2g
+
+using namespace p2g;
+
+extern "C" {
+
+const char *p2g_last_error(void) { return g_last_error.c_str(); }
+
+int p2g_strategy_info(const char **name, int *priority, int *available)
+{
+    if (name)
+        *name = "CUDA-sm100a";
+    if (priority)
+        *priority = P2G_PRIORITY_OPTIMAL;
+    if (available) {
+        int n = 0, ok = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) {
+            (void)cudaGetLastError();
+            n = 0;
+        }
+        for (int d = 0; d < n; ++d) {
+            int major = 0;
+            if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) ==
+                    cudaSuccess &&
+                major == 10)
+                ok = 1;
+        }
+        *available = ok;
+    }
+    return P2G_OK;
+}
+
+int p2g_create(int device, p2g_ctx **out)
+{
+    clear_error();
+    if (!out) {
+        set_error("p2g_create: null output pointer");
+        return P2G_EINVAL;
+    }
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        (void)cudaGetLastError();
+        set_error("p2g_create: no CUDA device %d", device);
+        return P2G_ENODEV;
+    }
+    cudaDeviceProp prop;
+    P2G_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        set_error("p2g_create: device %d is sm_%d%d, this build targets sm_100a", device,
+                  prop.major, prop.minor);
+        return P2G_ENODEV;
+    }
+    P2G_CUDA(cudaSetDevice(device));
+    p2g_ctx *ctx = new p2g_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->hparams.pinned = true;
+    int rc = P2G_OK;
+    do {
+        if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            set_error("cudaStreamCreate failed");
+            rc = P2G_ECUDA;
+            break;
+        }
+        ctx->stream = ctx->own_stream;
+        bool ev_ok = true;
+        for (cudaEvent_t &e : ctx->ev)
+            ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
+        if (!ev_ok) {
+            set_error("cudaEventCreate failed");
+            rc = P2G_ECUDA;
+            break;
+        }
+        const HostTables &t = tables();
+        if (cudaMalloc(&ctx->d_log, sizeof t.log) != cudaSuccess ||
+            cudaMalloc(&ctx->d_exp, sizeof t.exp) != cudaSuccess ||
+            cudaMemcpy(ctx->d_log, t.log, sizeof t.log, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(ctx->d_exp, t.exp, sizeof t.exp, cudaMemcpyHostToDevice) != cudaSuccess) {
+            set_error("p2g_create: GF table upload failed");
+            rc = P2G_ENOMEM;
+            break;
+        }
+    } while (0);
+    if (rc != P2G_OK) {
+        (void)cudaGetLastError();
+        p2g_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return P2G_OK;
+}
+
+int p2g_destroy(p2g_ctx *ctx)
+{
+    if (!ctx)
+        return P2G_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream)
+        cudaStreamSynchronize(ctx->own_stream);
+    ctx->planes.release();
+    ctx->recs.release();
+    ctx->in_copy.release();
+    ctx->out_copy.release();
+    ctx->params.release();
+    ctx->hparams.release();
+    ctx->coeffs.release();
+    ctx->recs2.release();
+    ctx->rhs.release();
+    ctx->inv.release();
+    ctx->gj_M.release();
+    ctx->gj_status.release();
+    if (ctx->d_log)
+        cudaFree(ctx->d_log);
+    if (ctx->d_exp)
+        cudaFree(ctx->d_exp);
+    for (cudaEvent_t e : ctx->ev)
+        if (e)
+            cudaEventDestroy(e);
+    if (ctx->own_stream)
+        cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return P2G_OK;
+}
+
+int p2g_set_stream(p2g_ctx *ctx, void *cuda_stream)
+{
+    clear_error();
+    if (!ctx) {
+        set_error("p2g_set_stream: null context");
+        return P2G_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
+    return P2G_OK;
+}
+
+int p2g_set_timing(p2g_ctx *ctx, int enable)
+{
+    clear_error();
+    if (!ctx) {
+        set_error("p2g_set_timing: null context");
+        return P2G_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->timing = enable != 0;
+    return P2G_OK;
+}
+
+int p2g_last_timing(p2g_ctx *ctx, p2g_timing *out)
+{
+    clear_error();
+    if (!ctx || !out) {
+        set_error("p2g_last_timing: null argument");
+        return P2G_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    *out = ctx->last;
+    return P2G_OK;
+}
+
+int p2g_par2_constants(size_t k, uint16_t *out)
+{
+    clear_error();
+    if (!out && k) {
+        set_error("p2g_par2_constants: null output");
+        return P2G_EINVAL;
+    }
+    par2_constants(k, out);
+    return P2G_OK;
+}
+
+int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_bytes,
+               const uint32_t *exps, size_t r, uint8_t *const *out, uint32_t flags)
+{
+    clear_error();
+    if (!ctx || (k && !src) || (r && (!out || !exps))) {
+        set_error("p2g_encode: null argument");
+        return P2G_EINVAL;
+    }
+    if (slice_bytes == 0 || slice_bytes % 2) {
+        set_error("p2g_encode: slice size %zu must be even and non-zero "
+                  "(\"Block size must be multiple of 2\", par2_rs.rs:697-699)",
+                  slice_bytes);
+        return P2G_EINVAL;
+    }
+    if (k > 65535 || r > 65535) {
+        set_error("p2g_encode: %zu inputs / %zu outputs exceed the GF(2^16) limit of 65535", k,
+                  r);
+        return P2G_ERANGE;
+    }
+    if (r == 0)
+        return P2G_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    begin(ctx);
+    const bool dev = flags & P2G_DEVICE_PTRS;
+    std::vector<uint8_t *> s, d;
+    bool s_staged = false, d_staged = false;
+    P2G_TRY(stage(ctx, ctx->in_copy, src, k, slice_bytes, dev, true, s, s_staged));
+    P2G_TRY(stage(ctx, ctx->out_copy, out, r, slice_bytes, dev, false, d, d_staged));
+    ParamLayout L(k, r, k * 2, r * 4);
+    P2G_TRY(ctx->hparams.ensure(L.total));
+    P2G_TRY(ctx->params.ensure(L.total));
+    uint8_t *h = ctx->hparams.as<uint8_t>();
+    memcpy(h + L.src_off, s.data(), k * sizeof(void *));
+    memcpy(h + L.dst_off, d.data(), r * sizeof(void *));
+    par2_constants(k, reinterpret_cast<uint16_t *>(h + L.a_off));
+    memcpy(h + L.b_off, exps, r * 4);
+    P2G_TRY(upload_params(ctx, L));
+    uint8_t *dp = ctx->params.as<uint8_t>();
+    P2G_TRY(ctx->recs.ensure(k * r * 64));
+    P2G_TRY(records_par2(ctx, reinterpret_cast<const uint16_t *>(dp + L.a_off),
+                         reinterpret_cast<const uint32_t *>(dp + L.b_off), static_cast<int>(k),
+                         static_cast<int>(r), ctx->recs.as<uint32_t>()));
+    P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.src_off),
+                       static_cast<int>(k), reinterpret_cast<uint8_t *const *>(dp + L.dst_off),
+                       static_cast<int>(r), slice_bytes, ctx->recs.as<uint32_t>(), 0));
+    if (d_staged)
+        P2G_TRY(unstage(ctx, out, d, r, slice_bytes, dev));
+    return finish(ctx);
+}
+
+int p2g_muladd_region(p2g_ctx *ctx, uint16_t *const *dsts, size_t ndst,
+                      const uint16_t *const *srcs, size_t nsrc,
+                      const uint16_t *const *coeff_rows, size_t off_u16, size_t len_u16,
+                      uint32_t flags)
+{
+    clear_error();
+    if (!ctx || (ndst && (!dsts || !coeff_rows)) || (nsrc && !srcs)) {
+        set_error("p2g_muladd_region: null argument");
+        return P2G_EINVAL;
+    }
+    if (ndst > 65535 || nsrc > 65535) {
+        set_error("p2g_muladd_region: too many slices");
+        return P2G_ERANGE;
+    }
+    if (ndst == 0 || nsrc == 0 || len_u16 == 0)
+        return P2G_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    begin(ctx);
+    const bool dev = flags & P2G_DEVICE_PTRS;
+    const size_t bytes = len_u16 * 2;
+    std::vector<const uint8_t *> sp(nsrc);
+    std::vector<uint8_t *> dp(ndst);
+    for (size_t i = 0; i < nsrc; ++i)
+        sp[i] = reinterpret_cast<const uint8_t *>(srcs[i] + off_u16);
+    for (size_t o = 0; o < ndst; ++o)
+        dp[o] = reinterpret_cast<uint8_t *>(dsts[o] + off_u16);
+    std::vector<uint16_t> coeff(ndst * nsrc);
+    for (size_t o = 0; o < ndst; ++o)
+        memcpy(&coeff[o * nsrc], coeff_rows[o], nsrc * 2);
+    std::vector<uint8_t *> s, d;
+    bool s_staged = false, d_staged = false;
+    P2G_TRY(stage(ctx, ctx->in_copy, sp.data(), nsrc, bytes, dev, true, s, s_staged));
+    P2G_TRY(stage(ctx, ctx->out_copy, dp.data(), ndst, bytes, dev, true, d, d_staged));
+    P2G_TRY(matrix_muladd(ctx, s, d, coeff.data(), bytes, 1));
+    if (d_staged)
+        P2G_TRY(unstage(ctx, dp.data(), d, ndst, bytes, dev));
+    return finish(ctx);
+}
+
+int p2g_muladd(p2g_ctx *ctx, uint16_t *dst, const uint16_t *src, size_t n, uint16_t c,
+               uint32_t flags)
+{
+    if (c == 0 || n == 0) {
+        clear_error();
+        return ctx ? P2G_OK : P2G_EINVAL;
+    }
+    const uint16_t *row = &c;
+    return p2g_muladd_region(ctx, &dst, 1, &src, 1, &row, 0, n, flags);
+}
+
+int p2g_mul_slice(p2g_ctx *ctx, uint16_t c, uint16_t *data, size_t n, uint32_t flags)
+{
+    clear_error();
+    if (!ctx || (n && !data)) {
+        set_error("p2g_mul_slice: null argument");
+        return P2G_EINVAL;
+    }
+    if (n == 0)
+        return P2G_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    begin(ctx);
+    const bool dev = flags & P2G_DEVICE_PTRS;
+    const size_t bytes = n * 2;
+    const uint8_t *in = reinterpret_cast<const uint8_t *>(data);
+    std::vector<uint8_t *> s;
+    bool staged = false;
+    P2G_TRY(stage(ctx, ctx->in_copy, &in, 1, bytes, dev, true, s, staged));
+    // in place: the planes are taken before the product is stored
+    P2G_TRY(matrix_muladd(ctx, s, s, &c, bytes, 0));
+    if (staged) {
+        uint8_t *user = reinterpret_cast<uint8_t *>(data);
+        P2G_TRY(unstage(ctx, &user, s, 1, bytes, dev));
+    }
+    return finish(ctx);
+}
+
+int p2g_invert(p2g_ctx *ctx, size_t m, const uint16_t *A, uint16_t *inv)
+{
+    clear_error();
+    if (!ctx || (m && (!A || !inv))) {
+        set_error("p2g_invert: null argument");
+        return P2G_EINVAL;
+    }
+    if (m > 65535) {
+        set_error("p2g_invert: m = %zu beyond 65535", m);
+        return P2G_ERANGE;
+    }
+    if (m == 0)
+        return P2G_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    begin(ctx);
+    P2G_TRY(ctx->coeffs.ensure(m * m * 2));
+    P2G_TRY(ctx->inv.ensure(m * m * 2));
+    P2G_CUDA(cudaMemcpyAsync(ctx->coeffs.p, A, m * m * 2, cudaMemcpyHostToDevice, ctx->stream));
+    GjWork w{ctx->gj_M, ctx->gj_status};
+    P2G_TRY(gj_invert(ctx, w, static_cast<int>(m), nullptr, nullptr, ctx->coeffs.as<uint16_t>(),
+                      ctx->inv.as<uint16_t>()));
+    int singular = 0;
+    P2G_TRY(gj_status(ctx, w, &singular));
+    if (singular) {
+        set_error("Singular matrix");
+        return P2G_ESINGULAR;
+    }
+    P2G_CUDA(cudaMemcpyAsync(inv, ctx->inv.p, m * m * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    return finish(ctx);
+}
+
+static int check_missing(size_t k, const uint64_t *missing, size_t m)
+{
+    for (size_t j = 0; j < m; ++j) {
+        if (missing[j] >= k || (j && missing[j] <= missing[j - 1])) {
+            set_error("missing indices must be strictly ascending and below k = %zu", k);
+            return P2G_EINVAL;
+        }
+    }
+    return P2G_OK;
+}
+
+int p2g_reconstruction_matrix(p2g_ctx *ctx, size_t k, const uint64_t *missing, size_t m,
+                              const uint32_t *exps, uint16_t *inv)
+{
+    clear_error();
+    if (!ctx || (m && (!missing || !exps || !inv))) {
+        set_error("p2g_reconstruction_matrix: null argument");
+        return P2G_EINVAL;
+    }
+    if (k > 65535 || m > k) {
+        set_error("p2g_reconstruction_matrix: k = %zu, m = %zu out of range", k, m);
+        return P2G_ERANGE;
+    }
+    P2G_TRY(check_missing(k, missing, m));
+    if (m == 0)
+        return P2G_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    begin(ctx);
+    std::vector<uint16_t> c(k);
+    par2_constants(k, c.data());
+    ParamLayout L(0, 0, m * 2, m * 4);
+    P2G_TRY(ctx->hparams.ensure(L.total));
+    P2G_TRY(ctx->params.ensure(L.total));
+    uint8_t *h = ctx->hparams.as<uint8_t>();
+    for (size_t j = 0; j < m; ++j)
+        reinterpret_cast<uint16_t *>(h + L.a_off)[j] = c[missing[j]];
+    memcpy(h + L.b_off, exps, m * 4);
+    P2G_TRY(upload_params(ctx, L));
+    uint8_t *dp = ctx->params.as<uint8_t>();
+    P2G_TRY(ctx->inv.ensure(m * m * 2));
+    GjWork w{ctx->gj_M, ctx->gj_status};
+    P2G_TRY(gj_invert(ctx, w, static_cast<int>(m), reinterpret_cast<const uint16_t *>(dp + L.a_off),
+                      reinterpret_cast<const uint32_t *>(dp + L.b_off), nullptr,
+                      ctx->inv.as<uint16_t>()));
+    int singular = 0;
+    P2G_TRY(gj_status(ctx, w, &singular));
+    if (singular) {
+        set_error("Singular matrix");
+        return P2G_ESINGULAR;
+    }
+    P2G_CUDA(cudaMemcpyAsync(inv, ctx->inv.p, m * m * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    return finish(ctx);
+}
+
+int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missing, size_t m,
+               const uint8_t *const *present, const uint32_t *exps,
+               const uint8_t *const *recovery, uint8_t *const *out, uint32_t flags)
+{
+    clear_error();
+    if (!ctx || (m && (!missing || !exps || !recovery || !out)) || (k > m && !present)) {
+        set_error("p2g_repair: null argument");
+        return P2G_EINVAL;
+    }
+    if (slice_bytes == 0 || slice_bytes % 2) {
+        set_error("p2g_repair: slice size %zu must be even and non-zero", slice_bytes);
+        return P2G_EINVAL;
+    }
+    if (k > 65535 || m > k) {
+        set_error("p2g_repair: k = %zu, m = %zu out of range", k, m);
+        return P2G_ERANGE;
+    }
+    P2G_TRY(check_missing(k, missing, m));
+    if (m == 0)
+        return P2G_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    begin(ctx);
+    const bool dev = flags & P2G_DEVICE_PTRS;
+    const size_t np = k - m;
+    std::vector<uint16_t> c(k);
+    par2_constants(k, c.data());
+    std::vector<uint16_t> cpres, cmiss(m);
+    cpres.reserve(np);
+    {
+        size_t j = 0;
+        for (size_t i = 0; i < k; ++i) {
+            if (j < m && missing[j] == i)
+                cmiss[j++] = c[i];
+            else
+                cpres.push_back(c[i]);
+        }
+    }
+    // slices: present data and recovery inputs, outputs
+    std::vector<uint8_t *> ps, os;
+    bool p_st = false, o_st = false;
+    P2G_TRY(stage(ctx, ctx->in_copy, present, np, slice_bytes, dev, true, ps, p_st));
+    // the right-hand sides start as copies of the recovery slices
+    const size_t slot = round16(slice_bytes);
+    P2G_TRY(ctx->rhs.ensure(slot * m));
+    std::vector<uint8_t *> rhs(m);
+    for (size_t j = 0; j < m; ++j) {
+        rhs[j] = ctx->rhs.as<uint8_t>() + j * slot;
+        P2G_CUDA(cudaMemcpyAsync(rhs[j], recovery[j], slice_bytes,
+                                 dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    }
+    P2G_TRY(stage(ctx, ctx->out_copy, out, m, slice_bytes, dev, false, os, o_st));
+    // parameter block: [present ptrs][rhs ptrs | out ptrs][cmiss | exps | cpres]
+    ParamLayout L(np, 2 * m, m * 2 + m * 4 + 16, np * 2);
+    P2G_TRY(ctx->hparams.ensure(L.total));
+    P2G_TRY(ctx->params.ensure(L.total));
+    uint8_t *h = ctx->hparams.as<uint8_t>();
+    memcpy(h + L.src_off, ps.data(), np * sizeof(void *));
+    memcpy(h + L.dst_off, rhs.data(), m * sizeof(void *));
+    memcpy(h + L.dst_off + m * sizeof(void *), os.data(), m * sizeof(void *));
+    const size_t exps_off = L.a_off + round16(m * 2);
+    memcpy(h + L.a_off, cmiss.data(), m * 2);
+    memcpy(h + exps_off, exps, m * 4);
+    if (np)
+        memcpy(h + L.b_off, cpres.data(), np * 2);
+    P2G_TRY(upload_params(ctx, L));
+    uint8_t *dp = ctx->params.as<uint8_t>();
+    const uint32_t *d_exps = reinterpret_cast<const uint32_t *>(dp + exps_off);
+    // 1. A^-1 on the device
+    P2G_TRY(ctx->inv.ensure(m * m * 2));
+    GjWork w{ctx->gj_M, ctx->gj_status};
+    P2G_TRY(gj_invert(ctx, w, static_cast<int>(m), reinterpret_cast<const uint16_t *>(dp + L.a_off),
+                      d_exps, nullptr, ctx->inv.as<uint16_t>()));
+    int singular = 0;
+    P2G_TRY(gj_status(ctx, w, &singular));
+    if (singular) {
+        set_error("Singular matrix");
+        return P2G_ESINGULAR;
+    }
+    // 2. RHS = R ^ V * present
+    if (np) {
+        P2G_TRY(ctx->recs.ensure(np * m * 64));
+        P2G_TRY(records_par2(ctx, reinterpret_cast<const uint16_t *>(dp + L.b_off), d_exps,
+                             static_cast<int>(np), static_cast<int>(m), ctx->recs.as<uint32_t>()));
+        P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.src_off),
+                           static_cast<int>(np),
+                           reinterpret_cast<uint8_t *const *>(dp + L.dst_off),
+                           static_cast<int>(m), slice_bytes, ctx->recs.as<uint32_t>(), 1));
+    }
+    // 3. missing = A^-1 * RHS
+    P2G_TRY(ctx->recs2.ensure(m * m * 64));
+    P2G_TRY(records_from_matrix(ctx, ctx->inv.as<uint16_t>(), static_cast<int>(m),
+                                static_cast<int>(m), ctx->recs2.as<uint32_t>()));
+    P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.dst_off),
+                       static_cast<int>(m),
+                       reinterpret_cast<uint8_t *const *>(dp + L.dst_off + m * sizeof(void *)),
+                       static_cast<int>(m), slice_bytes, ctx->recs2.as<uint32_t>(), 0));
+    if (o_st)
+        P2G_TRY(unstage(ctx, out, os, m, slice_bytes, dev));
+    return finish(ctx);
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// common.cuh -- context, scratch buffers and error plumbing shared by the
+// CUDA translation units of libpar2gpu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/par2gpu.h"
+
+namespace p2g {
+
+// Thread-local message behind p2g_last_error().
+void set_error(const char *fmt, ...);
+void clear_error();
+
+// Growable device (or pinned host) buffer owned by a context.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    bool pinned = false;
+    int ensure(size_t n);  // P2G_OK / P2G_ENOMEM; contents not preserved
+    void release();
+    template <class T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+}  // namespace p2g
+
+struct p2g_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t own_stream = nullptr;  // created with the context
+    cudaStream_t stream = nullptr;      // where work runs (own or caller's)
+    std::mutex mu;
+    // optional per-phase timing (p2g_set_timing / p2g_last_timing)
+    bool timing = false;
+    cudaEvent_t ev[5] = {};
+    bool ev_marked[5] = {};
+    int launches = 0;
+    p2g_timing last = {};
+    // Records event `idx` (0 call start, 1 records done, 2 planes done,
+    // 3 muladd done, 4 call end) when timing is enabled.
+    void mark(int idx)
+    {
+        if (timing && ev[idx]) {
+            cudaEventRecord(ev[idx], stream);
+            ev_marked[idx] = true;
+        }
+    }
+    // GF(2^16) log / antilog tables on the device (galois/core.rs:49-91)
+    uint16_t *d_log = nullptr;
+    uint16_t *d_exp = nullptr;
+    // scratch
+    p2g::DevBuf planes;    // bit-sliced inputs
+    p2g::DevBuf recs;      // coefficient records
+    p2g::DevBuf in_copy;   // device copies of host / misaligned inputs
+    p2g::DevBuf out_copy;  // device copies of host / misaligned outputs
+    p2g::DevBuf params;    // small device parameter block (pointer arrays ...)
+    p2g::DevBuf hparams;   // pinned host mirror of `params`
+    p2g::DevBuf coeffs;    // coefficient matrices
+    p2g::DevBuf recs2;     // records of a second pass (repair)
+    p2g::DevBuf rhs;       // repair right-hand sides
+    p2g::DevBuf inv;       // decode matrix
+    p2g::DevBuf gj_M;      // Gauss-Jordan augmented matrix
+    p2g::DevBuf gj_status; // Gauss-Jordan status + pivots
+};
+
+#define P2G_CUDA(call)                                                                  \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            p2g::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),      \
+                           __FILE__, __LINE__);                                         \
+            return P2G_ECUDA;                                                           \
+        }                                                                               \
+    } while (0)
+
+#define P2G_TRY(expr)           \
+    do {                        \
+        int rc_ = (expr);       \
+        if (rc_ != P2G_OK)      \
+            return rc_;         \
+    } while (0)

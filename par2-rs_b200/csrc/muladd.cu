@@ -1,0 +1,479 @@
+// muladd.cu -- GF(2^16) region multiply-accumulate on sm_100a.
+//
+// Replaces the per-strategy region kernels of par2-rs (galois/simd/x86/
+// avx2.rs:686-821 behind galois/region/mod.rs:90-131, and the column path
+// galois/mod.rs:328-349 used by par2_rs.rs:816-870) for both recovery-slice
+// creation and repair:
+//
+//     dst[o][x] (^)= XOR_i  coeff(i, o) * src[i][x]      (GF(2^16), 0x1100B)
+//
+// Design (bit-sliced tables, "method of four Russians" over GF(2)):
+//   * Inputs are first converted to 16 bit planes per group of 32 symbols
+//     (slices_to_planes).  Multiplication by a constant is GF(2)-linear on the
+//     planes (bitslice.cuh).
+//   * A CTA owns one column tile of 1024 symbols (2 KiB of every slice) and a
+//     block of up to 8*EREG outputs; each warp keeps EREG outputs x 16 planes
+//     in registers, lane L owning symbol group L of the tile.
+//   * Per input slice the CTA builds, in shared memory, two 256-row tables of
+//     every XOR combination of planes 0-7 and of planes 8-15 (64 KiB, lane L's
+//     column in bank L).  One output plane of one coefficient is then two
+//     conflict-free table reads and one XOR; the table rows to read are the
+//     coefficient's "record" (16 words), the same for all 32 lanes.
+//   * The next input's planes and records stream into a 4-slot shared-memory
+//     ring with cp.async while the current table is consumed; the table is
+//     double-buffered, one CTA barrier per input slice.
+//   * Few tiles / outputs: the input range is split across CTAs and the
+//     partial sums are folded into the output with atomic XOR.
+#include <algorithm>
+
+#include "bitslice.cuh"
+#include "muladd.cuh"
+
+namespace p2g {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr int kTileBytes = 2048;             // 1024 symbols
+constexpr int kTableWords = 512 * 32;        // T0 and T1, 128 B per row
+constexpr int kTableBytes = kTableWords * 4; // 64 KiB
+constexpr int kRing = 4;
+constexpr int kMaxEreg = 13;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// 32 little-endian u16 symbols at byte offset `off` of a 16-byte aligned
+// slice of S bytes (zero beyond S), as 16 words of two symbols each.
+__device__ __forceinline__ void load_group(const uint8_t *base, size_t S, size_t off,
+                                           uint32_t x[16])
+{
+    if (off + 64 <= S) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(base + off);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint4 v = __ldg(p + q);
+            x[4 * q] = v.x;
+            x[4 * q + 1] = v.y;
+            x[4 * q + 2] = v.z;
+            x[4 * q + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            size_t o = off + 4 * j;
+            uint32_t v = 0;
+            if (o + 4 <= S)
+                v = *reinterpret_cast<const uint32_t *>(base + o);
+            else if (o + 2 <= S)
+                v = *reinterpret_cast<const uint16_t *>(base + o);
+            x[j] = v;
+        }
+    }
+}
+
+// Writes (mode 0), XORs (mode 1) or atomically XORs (mode 2) 32 symbols.
+__device__ __forceinline__ void store_group(uint8_t *base, size_t S, size_t off,
+                                            const uint32_t x[16], int mode)
+{
+    if (mode == 2) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            size_t o = off + 4 * j;
+            if (o + 4 <= S) {
+                atomicXor(reinterpret_cast<unsigned int *>(base + o), x[j]);
+            } else if (o + 2 <= S) {
+                // o is 4-byte aligned: the low half of the aligned word
+                atomicXor(reinterpret_cast<unsigned int *>(base + o), x[j] & 0xFFFFu);
+            }
+        }
+        return;
+    }
+    if (off + 64 <= S) {
+        uint4 *p = reinterpret_cast<uint4 *>(base + off);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint4 v = make_uint4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+            if (mode == 1) {
+                uint4 old = p[q];
+                v.x ^= old.x;
+                v.y ^= old.y;
+                v.z ^= old.z;
+                v.w ^= old.w;
+            }
+            p[q] = v;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            size_t o = off + 4 * j;
+            if (o + 4 <= S) {
+                uint32_t *p = reinterpret_cast<uint32_t *>(base + o);
+                *p = mode == 1 ? (*p ^ x[j]) : x[j];
+            } else if (o + 2 <= S) {
+                uint16_t *p = reinterpret_cast<uint16_t *>(base + o);
+                uint16_t v = static_cast<uint16_t>(x[j]);
+                *p = mode == 1 ? static_cast<uint16_t>(*p ^ v) : v;
+            }
+        }
+    }
+}
+
+// LE symbols -> planes[i][t][b][lane]; one thread per group of 32 symbols.
+__global__ void slices_to_planes(const uint8_t *const *__restrict__ src, int nin, int T,
+                                 size_t S, uint32_t *__restrict__ planes)
+{
+    size_t gid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    size_t total = static_cast<size_t>(nin) * T * 32;
+    if (gid >= total)
+        return;
+    int lane = static_cast<int>(gid & 31);
+    size_t it = gid >> 5;
+    int t = static_cast<int>(it % T);
+    int i = static_cast<int>(it / T);
+    uint32_t x[16];
+    load_group(src[i], S, static_cast<size_t>(t) * kTileBytes + lane * 64, x);
+    transpose16x2(x);
+    uint32_t *P = planes + it * 512 + lane;
+#pragma unroll
+    for (int b = 0; b < 16; ++b)
+        P[b * 32] = x[b];
+}
+
+__device__ __forceinline__ void put_record(uint32_t *recs, size_t idx, uint32_t c)
+{
+    uint32_t w[16];
+    make_record(c, w);
+    uint4 *R = reinterpret_cast<uint4 *>(recs + idx * 16);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        R[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+}
+
+__global__ void records_matrix_kernel(const uint16_t *__restrict__ coeff, int nin, int nout,
+                                      uint32_t *__restrict__ recs)
+{
+    size_t gid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gid >= static_cast<size_t>(nin) * nout)
+        return;
+    int o = static_cast<int>(gid % nout);
+    size_t i = gid / nout;
+    put_record(recs, gid, coeff[static_cast<size_t>(o) * nin + i]);
+}
+
+// c_i^e by the log / antilog tables: (log c * e) mod 65535 (galois/core.rs:242-258)
+__global__ void records_par2_kernel(const uint16_t *__restrict__ consts,
+                                    const uint32_t *__restrict__ exps,
+                                    const uint16_t *__restrict__ glog,
+                                    const uint16_t *__restrict__ gexp, int nin, int nout,
+                                    uint32_t *__restrict__ recs)
+{
+    size_t gid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gid >= static_cast<size_t>(nin) * nout)
+        return;
+    int o = static_cast<int>(gid % nout);
+    int i = static_cast<int>(gid / nout);
+    uint32_t base = consts[i];
+    uint32_t e = exps[o];
+    uint32_t c;
+    if (base == 0)
+        c = e == 0 ? 1u : 0u;
+    else if (e == 0)
+        c = 1u;
+    else
+        c = gexp[static_cast<uint32_t>((static_cast<uint64_t>(glog[base]) * e) % 65535u)];
+    put_record(recs, gid, c);
+}
+
+template <int EREG>
+__global__ void __launch_bounds__(kThreads, 1)
+    muladd_bitsliced(const uint32_t *__restrict__ planes, const uint32_t *__restrict__ recs,
+                     int nin, int nout, int T, int nblk, int nsplit,
+                     uint8_t *const *__restrict__ dst, size_t S, int mode)
+{
+    constexpr int EBLK = kWarps * EREG;
+    constexpr int SLOT = kTileBytes + EBLK * 64;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint32_t *tab = reinterpret_cast<uint32_t *>(smem);
+    uint8_t *ring = smem + 2 * kTableBytes;
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    int bid = blockIdx.x;
+    const int split = bid % nsplit;
+    bid /= nsplit;
+    const int ob = bid % nblk;
+    const int t = bid / nblk;
+    const int obase = ob * EBLK;
+    const int nb = min(EBLK, nout - obase);
+    const int i0 = static_cast<int>(static_cast<long long>(nin) * split / nsplit);
+    const int i1 = static_cast<int>(static_cast<long long>(nin) * (split + 1) / nsplit);
+    const int my0 = warp * EREG;
+    const int myn = max(0, min(EREG, nb - my0));
+
+    auto issue = [&](int i) {
+        if (i < i1) {
+            uint8_t *s = ring + (i & (kRing - 1)) * SLOT;
+            const uint8_t *gp = reinterpret_cast<const uint8_t *>(
+                planes + (static_cast<size_t>(i) * T + t) * 512);
+            const uint8_t *gr = reinterpret_cast<const uint8_t *>(
+                recs + (static_cast<size_t>(i) * nout + obase) * 16);
+            const int nchunk = 128 + nb * 4;
+            for (int c = threadIdx.x; c < nchunk; c += kThreads) {
+                if (c < 128)
+                    cp_async16(s + c * 16, gp + c * 16);
+                else
+                    cp_async16(s + kTileBytes + (c - 128) * 16, gr + (c - 128) * 16);
+            }
+        }
+        cp_async_commit();
+    };
+
+    // Table rows [64*wq, 64*wq+64) of half `half` (planes 8*half .. 8*half+7).
+    auto build = [&](int i, int buf) {
+        const uint32_t *P = reinterpret_cast<const uint32_t *>(ring + (i & (kRing - 1)) * SLOT);
+        const int half = warp >> 2, wq = warp & 3;
+        uint32_t p[8];
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+            p[b] = P[(half * 8 + b) * 32 + lane];
+        uint32_t L[16];
+        L[0] = 0;
+        L[1] = p[0];
+        L[2] = p[1];
+        L[3] = p[0] ^ p[1];
+        L[4] = p[2];
+        L[5] = L[4] ^ p[0];
+        L[6] = L[4] ^ p[1];
+        L[7] = L[6] ^ p[0];
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+            L[8 + x] = L[x] ^ p[3];
+        uint32_t base = ((wq & 1) ? p[6] : 0u) ^ ((wq & 2) ? p[7] : 0u);
+        uint32_t H[4] = {base, base ^ p[4], base ^ p[5], base ^ p[4] ^ p[5]};
+        uint32_t *T0 = tab + buf * kTableWords + (half * 256 + wq * 64) * 32 + lane;
+#pragma unroll
+        for (int hh = 0; hh < 4; ++hh)
+#pragma unroll
+            for (int x = 0; x < 16; ++x)
+                T0[(hh * 16 + x) * 32] = H[hh] ^ L[x];
+    };
+
+    uint32_t acc[EREG][16];
+#pragma unroll
+    for (int e = 0; e < EREG; ++e)
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            acc[e][j] = 0;
+
+    auto consume = [&](int i, int buf) {
+        const uint4 *R = reinterpret_cast<const uint4 *>(ring + (i & (kRing - 1)) * SLOT +
+                                                         kTileBytes) +
+                         my0 * 4;
+        const char *tb = reinterpret_cast<const char *>(tab + buf * kTableWords + lane);
+#pragma unroll
+        for (int e = 0; e < EREG; ++e) {
+            if (e < myn) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint4 r = R[e * 4 + q];
+                    const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const uint32_t a = *reinterpret_cast<const uint32_t *>(tb + (w[k] & 0xFFFFu));
+                        const uint32_t b = *reinterpret_cast<const uint32_t *>(tb + (w[k] >> 16));
+                        acc[e][4 * q + k] ^= a ^ b;
+                    }
+                }
+            }
+        }
+    };
+
+    if (i0 < i1) {
+        issue(i0);
+        issue(i0 + 1);
+        issue(i0 + 2);
+        cp_async_wait<1>();
+        __syncthreads();
+        build(i0, 0);
+        __syncthreads();
+        for (int i = i0; i < i1; ++i) {
+            issue(i + 3);
+            if (i + 1 < i1)
+                build(i + 1, (i + 1 - i0) & 1);
+            consume(i, (i - i0) & 1);
+            cp_async_wait<1>();
+            __syncthreads();
+        }
+    }
+    cp_async_wait<0>();
+
+    const int smode = nsplit > 1 ? 2 : mode;
+#pragma unroll
+    for (int e = 0; e < EREG; ++e) {
+        if (e < myn) {
+            uint32_t x[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                x[j] = acc[e][j];
+            transpose16x2(x);
+            store_group(dst[obase + my0 + e], S, static_cast<size_t>(t) * kTileBytes + lane * 64,
+                        x, smode);
+        }
+    }
+}
+
+// Zeroes nout slices before a split (atomic-XOR) run in store mode.
+__global__ void zero_slices(uint8_t *const *__restrict__ dst, int nout, size_t S)
+{
+    int o = blockIdx.y;
+    if (o >= nout)
+        return;
+    uint8_t *d = dst[o];
+    for (size_t x = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 16; x < S;
+         x += static_cast<size_t>(gridDim.x) * blockDim.x * 16) {
+        if (x + 16 <= S)
+            *reinterpret_cast<uint4 *>(d + x) = make_uint4(0, 0, 0, 0);
+        else
+            for (size_t y = x; y < S; y += 2)
+                *reinterpret_cast<uint16_t *>(d + y) = 0;
+    }
+}
+
+using KernelFn = void (*)(const uint32_t *, const uint32_t *, int, int, int, int, int,
+                          uint8_t *const *, size_t, int);
+
+static KernelFn kernel_for(int ereg)
+{
+    switch (ereg) {
+    case 1: return muladd_bitsliced<1>;
+    case 2: return muladd_bitsliced<2>;
+    case 3: return muladd_bitsliced<3>;
+    case 4: return muladd_bitsliced<4>;
+    case 5: return muladd_bitsliced<5>;
+    case 6: return muladd_bitsliced<6>;
+    case 7: return muladd_bitsliced<7>;
+    case 8: return muladd_bitsliced<8>;
+    case 9: return muladd_bitsliced<9>;
+    case 10: return muladd_bitsliced<10>;
+    case 11: return muladd_bitsliced<11>;
+    case 12: return muladd_bitsliced<12>;
+    case 13: return muladd_bitsliced<13>;
+    default: return nullptr;
+    }
+}
+
+static size_t smem_bytes(int ereg)
+{
+    return 2 * kTableBytes + kRing * (kTileBytes + kWarps * ereg * 64);
+}
+
+MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t S)
+{
+    MuladdPlan p;
+    const int T = static_cast<int>((S + kTileBytes - 1) / kTileBytes);
+    p.nblk = (nout + kWarps * kMaxEreg - 1) / (kWarps * kMaxEreg);
+    p.ereg = (nout + kWarps * p.nblk - 1) / (kWarps * p.nblk);
+    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    const long long ctas = static_cast<long long>(T) * p.nblk;
+    // The atomic-XOR fold touches whole aligned words: only for S % 4 == 0.
+    if (ctas < 2LL * sms && S % 4 == 0) {
+        long long want = (2LL * sms + ctas - 1) / ctas;
+        long long cap = std::max(1, nin / 8);
+        p.nsplit = static_cast<int>(std::min(want, cap));
+    }
+    return p;
+}
+
+int records_from_matrix(p2g_ctx *ctx, const uint16_t *d_coeff, int nin, int nout,
+                        uint32_t *d_recs)
+{
+    size_t n = static_cast<size_t>(nin) * nout;
+    if (n == 0)
+        return P2G_OK;
+    records_matrix_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx->stream>>>(
+        d_coeff, nin, nout, d_recs);
+    P2G_CUDA(cudaGetLastError());
+    ++ctx->launches;
+    return P2G_OK;
+}
+
+int records_par2(p2g_ctx *ctx, const uint16_t *d_consts, const uint32_t *d_exps, int nin,
+                 int nout, uint32_t *d_recs)
+{
+    size_t n = static_cast<size_t>(nin) * nout;
+    if (n == 0)
+        return P2G_OK;
+    records_par2_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx->stream>>>(
+        d_consts, d_exps, ctx->d_log, ctx->d_exp, nin, nout, d_recs);
+    P2G_CUDA(cudaGetLastError());
+    ++ctx->launches;
+    return P2G_OK;
+}
+
+int muladd_run(p2g_ctx *ctx, const uint8_t *const *d_src, int nin, uint8_t *const *d_dst,
+               int nout, size_t S, const uint32_t *d_recs, int mode, const MuladdPlan *plan)
+{
+    if (nout <= 0)
+        return P2G_OK;
+    const int T = static_cast<int>((S + kTileBytes - 1) / kTileBytes);
+    MuladdPlan p = plan ? *plan : choose_plan(ctx, nin, nout, S);
+    if (p.ereg < 1 || p.ereg > kMaxEreg || p.nblk * kWarps * p.ereg < nout || p.nsplit < 1) {
+        set_error("invalid muladd plan ereg=%d nblk=%d nsplit=%d for %d outputs", p.ereg,
+                  p.nblk, p.nsplit, nout);
+        return P2G_EINVAL;
+    }
+    if (nin == 0) {
+        if (mode == 0) {
+            dim3 g(static_cast<unsigned>(std::min<size_t>((S + 4095) / 4096, 1024)), nout);
+            zero_slices<<<g, 256, 0, ctx->stream>>>(d_dst, nout, S);
+            P2G_CUDA(cudaGetLastError());
+            ++ctx->launches;
+        }
+        return P2G_OK;
+    }
+    size_t plane_bytes = static_cast<size_t>(nin) * T * kTileBytes;
+    P2G_TRY(ctx->planes.ensure(plane_bytes));
+    uint32_t *planes = ctx->planes.as<uint32_t>();
+    size_t groups = static_cast<size_t>(nin) * T * 32;
+    ctx->mark(1);
+    slices_to_planes<<<static_cast<unsigned>((groups + 255) / 256), 256, 0, ctx->stream>>>(
+        d_src, nin, T, S, planes);
+    P2G_CUDA(cudaGetLastError());
+    ++ctx->launches;
+    if (p.nsplit > 1 && mode == 0) {
+        dim3 g(static_cast<unsigned>(std::min<size_t>((S + 4095) / 4096, 1024)), nout);
+        zero_slices<<<g, 256, 0, ctx->stream>>>(d_dst, nout, S);
+        P2G_CUDA(cudaGetLastError());
+        ++ctx->launches;
+    }
+    KernelFn fn = kernel_for(p.ereg);
+    size_t smem = smem_bytes(p.ereg);
+    P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    long long grid = static_cast<long long>(T) * p.nblk * p.nsplit;
+    if (grid > 0x7fffffffLL) {
+        set_error("muladd grid too large");
+        return P2G_ERANGE;
+    }
+    ctx->mark(2);
+    fn<<<static_cast<unsigned>(grid), kThreads, smem, ctx->stream>>>(
+        planes, d_recs, nin, nout, T, p.nblk, p.nsplit, d_dst, S, mode);
+    P2G_CUDA(cudaGetLastError());
+    ++ctx->launches;
+    ctx->mark(3);
+    return P2G_OK;
+}
+
+}  // namespace p2g

@@ -1,0 +1,34 @@
+// muladd.cuh -- host launchers of the GF(2^16) region multiply-accumulate.
+#pragma once
+#include "common.cuh"
+
+namespace p2g {
+
+// How one muladd problem is cut into CTAs (chosen by choose_plan or by the
+// autotuner): outputs per warp, output blocks, input splits.
+struct MuladdPlan {
+    int ereg = 1;    // outputs per warp (accumulators: 16 registers each)
+    int nblk = 1;    // output blocks of 8*ereg outputs
+    int nsplit = 1;  // input ranges reduced with atomic XOR
+};
+
+MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t slice_bytes);
+
+// Coefficient records [nin][nout][16 words] from a row-major matrix
+// coeff[nout][nin] (coefficients[dst][src] of galois/region/mod.rs:78-82).
+int records_from_matrix(p2g_ctx *ctx, const uint16_t *d_coeff, int nin, int nout,
+                        uint32_t *d_recs);
+
+// Records of the PAR2 encoding matrix: coefficient (i, o) = consts[i]^exps[o]
+// (par2_rs.rs:707-719).
+int records_par2(p2g_ctx *ctx, const uint16_t *d_consts, const uint32_t *d_exps, int nin,
+                 int nout, uint32_t *d_recs);
+
+// dst[o] (^)= sum_i coeff(i, o) * src[i] over slices of slice_bytes.
+// d_src / d_dst are DEVICE arrays of 16-byte aligned device pointers.
+// mode 0 stores, mode 1 XORs into the existing contents.
+int muladd_run(p2g_ctx *ctx, const uint8_t *const *d_src, int nin, uint8_t *const *d_dst,
+               int nout, size_t slice_bytes, const uint32_t *d_recs, int mode,
+               const MuladdPlan *plan = nullptr);
+
+}  // namespace p2g

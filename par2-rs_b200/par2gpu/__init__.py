@@ -1,0 +1,195 @@
+"""Python front end of libpar2gpu, the sm_100a GF(2^16) erasure-coding library.
+
+The functions mirror the C ABI in include/par2gpu.h one to one (ctypes, no
+torch types in the signatures).  Device buffers may be torch CUDA tensors,
+whose data pointers are passed with ``device=True``.
+
+There is no CPU fallback: loading fails loudly when the shared library is
+missing, and every call raises ``Par2GpuError`` on a non-zero status.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libpar2gpu.so")
+
+OK = 0
+EINVAL = -1
+ENOMEM = -2
+ECUDA = -3
+ESINGULAR = -4
+ETIMEOUT = -5
+ENODEV = -6
+ERANGE = -7
+DEVICE_PTRS = 0x1
+PRIORITY_OPTIMAL = 40
+
+_CODES = {EINVAL: "EINVAL", ENOMEM: "ENOMEM", ECUDA: "ECUDA", ESINGULAR: "ESINGULAR",
+          ETIMEOUT: "ETIMEOUT", ENODEV: "ENODEV", ERANGE: "ERANGE"}
+
+# (name, restype, argtypes) of every exported entry point
+_P = ctypes.c_void_p
+_S = ctypes.c_size_t
+_I = ctypes.c_int
+_U32 = ctypes.c_uint32
+_U16 = ctypes.c_uint16
+SIGNATURES = [
+    ("p2g_last_error", ctypes.c_char_p, []),
+    ("p2g_create", _I, [_I, _P]),
+    ("p2g_destroy", _I, [_P]),
+    ("p2g_set_stream", _I, [_P, _P]),
+    ("p2g_set_timing", _I, [_P, _I]),
+    ("p2g_last_timing", _I, [_P, _P]),
+    ("p2g_strategy_info", _I, [_P, _P, _P]),
+    ("p2g_mul_slice", _I, [_P, _U16, _P, _S, _U32]),
+    ("p2g_muladd", _I, [_P, _P, _P, _S, _U16, _U32]),
+    ("p2g_muladd_region", _I, [_P, _P, _S, _P, _S, _P, _S, _S, _U32]),
+    ("p2g_par2_constants", _I, [_S, _P]),
+    ("p2g_encode", _I, [_P, _P, _S, _S, _P, _S, _P, _U32]),
+]
+
+
+class Timing(ctypes.Structure):
+    """p2g_timing: per-phase device milliseconds of the last call."""
+    _fields_ = [("ms_records", ctypes.c_float), ("ms_planes", ctypes.c_float),
+                ("ms_muladd", ctypes.c_float), ("ms_total", ctypes.c_float),
+                ("launches", ctypes.c_int)]
+
+
+class Par2GpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_CODES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libpar2gpu.so not built at {LIB_PATH}; run __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error():
+    return lib().p2g_last_error().decode(errors="replace")
+
+
+def check(rc):
+    if rc != OK:
+        raise Par2GpuError(rc, last_error())
+    return rc
+
+
+def strategy_info():
+    """(name, priority, available) as GaloisSimdStrategy::{name, priority,
+    is_available} (par2-rs galois/simd/mod.rs:26-33)."""
+    name = ctypes.c_char_p()
+    prio = ctypes.c_int()
+    avail = ctypes.c_int()
+    check(lib().p2g_strategy_info(ctypes.byref(name), ctypes.byref(prio), ctypes.byref(avail)))
+    return name.value.decode(), prio.value, bool(avail.value)
+
+
+def par2_constants(k):
+    out = np.zeros(k, np.uint16)
+    check(lib().p2g_par2_constants(k, out.ctypes.data))
+    return out
+
+
+def _ptr(x):
+    """Address of a numpy array, a torch tensor or a raw int."""
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return x.ctypes.data
+
+
+def _ptr_array(xs):
+    arr = (ctypes.c_void_p * max(1, len(xs)))(*[_ptr(x) for x in xs])
+    return arr
+
+
+class Context:
+    """One p2g_ctx bound to a CUDA device (p2g_create / p2g_destroy)."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        check(lib().p2g_create(device, ctypes.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            lib().p2g_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        """Run on a caller CUDA stream (int handle, e.g. torch's
+        ``cuda_stream``); None restores the context's own stream."""
+        check(lib().p2g_set_stream(self.h, stream or None))
+
+    def set_timing(self, enable=True):
+        check(lib().p2g_set_timing(self.h, 1 if enable else 0))
+
+    def last_timing(self):
+        t = Timing()
+        check(lib().p2g_last_timing(self.h, ctypes.byref(t)))
+        return t
+
+    # --- GaloisSimdStrategy mirror (galois/simd/mod.rs:36-58) -------------
+    def mul_slice(self, scalar, data, device=False):
+        n = data.numel() if hasattr(data, "numel") else data.size
+        check(lib().p2g_mul_slice(self.h, scalar, _ptr(data), n, DEVICE_PTRS if device else 0))
+
+    def muladd(self, dst, src, scalar, device=False):
+        n = dst.numel() if hasattr(dst, "numel") else dst.size
+        check(lib().p2g_muladd(self.h, _ptr(dst), _ptr(src), n, scalar,
+                               DEVICE_PTRS if device else 0))
+
+    def muladd_region(self, dsts, srcs, coeffs, region_offset, region_size, device=False):
+        """dsts[d][off:off+len] ^= sum_s coeffs[d][s] * srcs[s][off:off+len]
+        (u16 units); coeffs is a [ndst][nsrc] array."""
+        co = np.ascontiguousarray(coeffs, np.uint16).reshape(len(dsts), len(srcs))
+        rows = _ptr_array([co[d] for d in range(len(dsts))])
+        check(lib().p2g_muladd_region(self.h, _ptr_array(dsts), len(dsts), _ptr_array(srcs),
+                                      len(srcs), rows, region_offset, region_size,
+                                      DEVICE_PTRS if device else 0))
+
+    # --- coarse-grained encode (par2_rs.rs:687-902) -----------------------
+    def encode(self, srcs, slice_bytes, exps, outs, device=False):
+        e = np.ascontiguousarray(exps, np.uint32)
+        check(lib().p2g_encode(self.h, _ptr_array(srcs), len(srcs), slice_bytes, e.ctypes.data,
+                               len(e), _ptr_array(outs), DEVICE_PTRS if device else 0))
+
+    def encode_array(self, src, exps):
+        """Host convenience: src uint8 [k, S] -> recovery uint8 [r, S]."""
+        src = np.ascontiguousarray(src, np.uint8)
+        k, S = src.shape
+        out = np.zeros((len(exps), S), np.uint8)
+        self.encode([src[i] for i in range(k)], S, exps, [out[e] for e in range(len(exps))])
+        return out

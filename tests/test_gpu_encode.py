@@ -1,0 +1,131 @@
+"""GPU parity of the GF(2^16) multiply-accumulate (K1) through the C ABI
+against the oracle, bit-exact.
+
+Mirrors par2-rs's own strategy tests (src/galois/tests.rs:482-553: every
+strategy against the scalar path at sizes {7, 8, 15, 16, 31, 32, 100, 1024}
+x scalars {0, 1, 2, 12345, 65535}) and its fixture check
+(src/parser.rs:957-1021, here for all 60 QuickPar recovery slices).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests import quickpar
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import par2gpu
+
+    c = par2gpu.Context(0)
+    yield c
+    c.close()
+
+
+def test_strategy_available():
+    import par2gpu
+
+    name, prio, avail = par2gpu.strategy_info()
+    assert (name, prio, avail) == ("CUDA-sm100a", 40, True)
+
+
+SIZES = [7, 8, 15, 16, 31, 32, 100, 1024]
+SCALARS = [0, 1, 2, 12345, 65535]
+
+
+@pytest.mark.parametrize("size", SIZES)
+def test_mul_slice_and_muladd_sweep(ctx, size):
+    for scalar in SCALARS:
+        data = ((np.arange(size) * 97 + 1) & 0xFFFF).astype(np.uint16)
+        want = np.array([oracle.gf_mul(int(v), scalar) for v in data], np.uint16)
+        got = data.copy()
+        ctx.mul_slice(scalar, got)
+        assert np.array_equal(got, want), (size, scalar)
+
+        src = ((np.arange(size) * 13 + 7) & 0xFFFF).astype(np.uint16)
+        dst = ((np.arange(size) * 17 + 3) & 0xFFFF).astype(np.uint16)
+        want = dst ^ np.array([oracle.gf_mul(int(v), scalar) for v in src], np.uint16)
+        ctx.muladd(dst, src, scalar)
+        assert np.array_equal(dst, want), (size, scalar)
+
+
+def test_quickpar_recovery_slices(ctx):
+    qp = quickpar.load()
+    src, _ = qp.slices()
+    got = ctx.encode_array(src, np.arange(60, dtype=np.uint32))
+    for e in range(60):
+        assert np.array_equal(got[e], qp.recovery[e]), f"exponent {e}"
+
+
+@pytest.mark.parametrize("k,S,r", [
+    (1, 2, 1), (3, 6, 2), (5, 64, 3), (17, 2050, 5), (40, 4096, 13), (256, 65536 // 8, 13),
+    (64, 2048 * 3 + 34, 37), (33, 8192, 104), (20, 4096, 105), (12, 2048, 210),
+])
+def test_encode_matches_oracle(ctx, k, S, r):
+    rng = np.random.default_rng(k * 1000 + r)
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(r, dtype=np.uint32)
+    got = ctx.encode_array(src, exps)
+    want = oracle.encode(src, exps)
+    assert np.array_equal(got, want)
+
+
+def test_encode_sparse_exponents_and_zero_slices(ctx):
+    rng = np.random.default_rng(5)
+    src = rng.integers(0, 256, (30, 4096), dtype=np.uint8)
+    src[3] = 0
+    src[7, :100] = 0
+    exps = np.array([0, 5, 17, 65534, 1000, 2], np.uint32)
+    assert np.array_equal(ctx.encode_array(src, exps), oracle.encode(src, exps))
+
+
+def test_muladd_region_offsets(ctx):
+    rng = np.random.default_rng(11)
+    n = 5000
+    srcs = [rng.integers(0, 65536, n, dtype=np.uint16) for _ in range(9)]
+    dsts = [rng.integers(0, 65536, n, dtype=np.uint16) for _ in range(6)]
+    coeffs = rng.integers(0, 65536, (6, 9), dtype=np.uint16)
+    coeffs[2, 4] = 0
+    coeffs[5, :] = 0
+    want = [d.copy() for d in dsts]
+    oracle.muladd_region(want, srcs, coeffs, 129, 3001)
+    got = [d.copy() for d in dsts]
+    ctx.muladd_region(got, srcs, coeffs, 129, 3001)
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
+
+
+def test_device_pointers_aligned_and_misaligned(ctx):
+    import torch
+
+    rng = np.random.default_rng(21)
+    k, S, r = 19, 6144, 7
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(r, dtype=np.uint32)
+    want = oracle.encode(src, exps)
+    d_src = torch.from_numpy(src).cuda()
+    d_out = torch.zeros((r, S), dtype=torch.uint8, device="cuda")
+    ctx.encode([d_src[i] for i in range(k)], S, exps, [d_out[e] for e in range(r)], device=True)
+    assert np.array_equal(d_out.cpu().numpy(), want)
+    # 2-byte aligned device slices are staged internally
+    big = torch.zeros(k * (S + 2) + 2, dtype=torch.uint8, device="cuda")
+    views = [big[2 + i * (S + 2): 2 + i * (S + 2) + S] for i in range(k)]
+    for i in range(k):
+        views[i].copy_(d_src[i])
+    outbig = torch.zeros(r * (S + 2) + 2, dtype=torch.uint8, device="cuda")
+    oviews = [outbig[2 + e * (S + 2): 2 + e * (S + 2) + S] for e in range(r)]
+    ctx.encode(views, S, exps, oviews, device=True)
+    for e in range(r):
+        assert np.array_equal(oviews[e].cpu().numpy(), want[e])
+
+
+def test_bad_arguments_report_errors(ctx):
+    import par2gpu
+
+    src = np.zeros((2, 7), np.uint8)
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        ctx.encode([src[0], src[1]], 7, [0], [np.zeros(7, np.uint8)])
+    assert ei.value.code == par2gpu.EINVAL
+    assert "even" in par2gpu.last_error()
