@@ -39,8 +39,19 @@ import numpy as np  # noqa: E402
 
 METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] \
     if os.path.exists(os.path.join(ROOT, "BASELINE.json")) else "encode GB/s"
-K_SRC, SLICE, R_REC = 2048, 1 << 20, 205
-WORKLOAD = "large_encode: 4 files x 512 MiB seeded uniform random, 1 MiB slices, k=2048, r=205 (10%)"
+WORKLOADS = {
+    # the configuration the headline metric is quoted on
+    "large_encode": (2048, 1 << 20, 205,
+                     "large_encode: 4 files x 512 MiB seeded uniform random, 1 MiB slices, "
+                     "k=2048, r=205 (10%)"),
+    # the same shape with 128 KiB slices (256 MB of sources): small enough
+    # for an ncu --set full capture
+    "profile_encode": (2048, 128 << 10, 205,
+                       "profile_encode: k=2048 x 128 KiB seeded uniform random, r=205"),
+    # the CPU-runnable plain configuration: 16 MiB, 64 KiB slices, 5 %
+    "plain": (256, 64 << 10, 13, "plain: 1 file x 16 MiB, 64 KiB slices, k=256, r=13 (5%)"),
+}
+K_SRC, SLICE, R_REC, WORKLOAD = WORKLOADS["large_encode"]
 SEED = 20261203
 CPU_SAMPLE_BYTES = 48 * 1024  # columns of every slice in the CPU sample
 
@@ -233,6 +244,14 @@ def run_ours(args, rank, world):
     ctx.set_timing(False)
     value = world * k * S / (ms_step * 1e-3) / 1e9
 
+    if args.quick:
+        ctx.close()
+        if rank == 0:
+            print(json.dumps({"workload": WORKLOAD, "ms_per_step": ms_step, "value": value,
+                              "unit": "GB/s", "kernel_ms": sum(mul_ms) / len(mul_ms),
+                              "gpu_launches": launches, "clocks": clk}), flush=True)
+        return
+
     # ---- end to end through the C ABI with pinned host buffers (e2e) ----
     src_h = src_pinned.numpy()
     out_h = out_pinned.numpy()
@@ -313,7 +332,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="large_encode", choices=sorted(WORKLOADS))
+    ap.add_argument("--quick", action="store_true",
+                    help="device-resident timing only (no e2e, roofline probe or CPU baseline)")
     args = ap.parse_args()
+    global K_SRC, SLICE, R_REC, WORKLOAD
+    K_SRC, SLICE, R_REC, WORKLOAD = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -141,6 +141,20 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
                const uint8_t *const *present, const uint32_t *exps,
                const uint8_t *const *recovery, uint8_t *const *out, uint32_t flags);
 
+/* Per-slice MD5 (RFC 1321) and CRC-32/ISO-HDLC of n slices of slice_bytes
+ * each, the IFSC checksums par2-rs computes with the md-5 and crc32fast
+ * crates (creator.rs:397-409, hash/md5_crc32_fused.rs:28-88).  md5_out
+ * receives 16 bytes per slice, crc_out one value per slice (host arrays). */
+int p2g_hash_slices(p2g_ctx *ctx, const uint8_t *const *slices, size_t n, size_t slice_bytes,
+                    uint8_t *md5_out, uint32_t *crc_out, uint32_t flags);
+
+/* Slice verification of verify_file_blocks (verify.rs:610-648): ok_out[i] = 1
+ * when slice i has the expected CRC32 and the expected MD5, else 0 (the
+ * reference rejects on CRC before computing MD5; the verdict is the same). */
+int p2g_verify_slices(p2g_ctx *ctx, const uint8_t *const *slices, size_t n, size_t slice_bytes,
+                      const uint8_t *md5_expect, const uint32_t *crc_expect, uint8_t *ok_out,
+                      uint32_t flags);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,12 +65,24 @@ constexpr uint32_t kRowBytes = 128;
 
 // The 16-word "record" of a coefficient c.  The 16 input planes are split in
 // two halves of 8; for each half a 256-row table holds every XOR combination
-// of its planes (row n = XOR of the planes whose bit is set in n).  Output
-// plane j is then  T0[n0_j] ^ T1[n1_j]  with
-//   n0_j = sum_{b<8} bit_j(c x^b)     << b
-//   n1_j = sum_{b<8} bit_j(c x^{b+8}) << b.
-// Word j holds both row byte-offsets: low half n0_j*128, high half
-// (256+n1_j)*128 (T1 follows T0 in the same 64 KiB table).
+// of its planes (row n = XOR of the planes whose bit is set in n; T1 follows
+// T0, rows of 128 bytes: one word per lane).  Output plane j is then
+//   T0[n0_j] ^ T1[n1_j],  n0_j = sum_{b<8} bit_j(c x^b) << b,
+//                         n1_j = sum_{b<8} bit_j(c x^{b+8}) << b.
+// The rows are fetched four at a time with ldmatrix.x4 (matrix m's eight
+// 16-byte row pointers come from lanes 8m..8m+7, so lane L receives word L of
+// each of the four rows).  For plane pair p (planes 2p, 2p+1) the four rows are
+//   m = 0: T0[n0_2p]   m = 1: T1[n1_2p]   m = 2: T0[n0_2p+1]   m = 3: T1[n1_2p+1]
+// and word 4m + i of the record holds the byte offsets of matrix m's rows for
+// p = 2i (low half) and p = 2i+1 (high half), so lane L reads the 16 bytes at
+// word 4*(L/8) and needs no other record data.
+__host__ __device__ __forceinline__ uint32_t row_offset(int m, uint32_t n0[16], uint32_t n1[16],
+                                                        int p)
+{
+    const int j = 2 * p + (m >> 1);
+    return (m & 1) ? (256u + n1[j]) * kRowBytes : n0[j] * kRowBytes;
+}
+
 __host__ __device__ __forceinline__ void make_record(uint32_t c, uint32_t w[16])
 {
     uint32_t col[16];
@@ -80,16 +92,23 @@ __host__ __device__ __forceinline__ void make_record(uint32_t c, uint32_t w[16])
         col[b] = v;
         v = gf_times_x(v);
     }
+    uint32_t n0[16], n1[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-        uint32_t n0 = 0, n1 = 0;
+        uint32_t a = 0, b1 = 0;
 #pragma unroll
         for (int b = 0; b < 8; ++b) {
-            n0 |= ((col[b] >> j) & 1u) << b;
-            n1 |= ((col[b + 8] >> j) & 1u) << b;
+            a |= ((col[b] >> j) & 1u) << b;
+            b1 |= ((col[b + 8] >> j) & 1u) << b;
         }
-        w[j] = (n0 * kRowBytes) | (((256u + n1) * kRowBytes) << 16);
+        n0[j] = a;
+        n1[j] = b1;
     }
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            w[4 * m + i] = row_offset(m, n0, n1, 2 * i) | (row_offset(m, n0, n1, 2 * i + 1) << 16);
 }
 
 }  // namespace p2g

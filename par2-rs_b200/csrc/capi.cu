@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "hash.cuh"
 #include "invert.cuh"
 #include "muladd.cuh"
 
@@ -302,6 +303,14 @@ int p2g_create(int device, p2g_ctx **out)
             rc = P2G_ENOMEM;
             break;
         }
+        static uint32_t crc_tab[4][256];
+        crc32_tables(crc_tab);
+        if (cudaMalloc(&ctx->d_crc, sizeof crc_tab) != cudaSuccess ||
+            cudaMemcpy(ctx->d_crc, crc_tab, sizeof crc_tab, cudaMemcpyHostToDevice) != cudaSuccess) {
+            set_error("p2g_create: CRC table upload failed");
+            rc = P2G_ENOMEM;
+            break;
+        }
     } while (0);
     if (rc != P2G_OK) {
         (void)cudaGetLastError();
@@ -337,6 +346,9 @@ int p2g_destroy(p2g_ctx *ctx)
         cudaFree(ctx->d_log);
     if (ctx->d_exp)
         cudaFree(ctx->d_exp);
+    if (ctx->d_crc)
+        cudaFree(ctx->d_crc);
+    ctx->hash_out.release();
     for (cudaEvent_t e : ctx->ev)
         if (e)
             cudaEventDestroy(e);
@@ -710,6 +722,84 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
     if (o_st)
         P2G_TRY(unstage(ctx, out, os, m, slice_bytes, dev));
     return finish(ctx);
+}
+
+static int hash_common(p2g_ctx *ctx, const uint8_t *const *slices, size_t n, size_t S,
+                       uint32_t flags, std::vector<uint8_t> &md5, std::vector<uint32_t> &crc)
+{
+    const bool dev = flags & P2G_DEVICE_PTRS;
+    std::vector<uint8_t *> sp;
+    bool staged = false;
+    P2G_TRY(stage(ctx, ctx->in_copy, slices, n, S, dev, true, sp, staged));
+    ParamLayout L(n, 0, 0, 0);
+    P2G_TRY(ctx->hparams.ensure(L.total));
+    P2G_TRY(ctx->params.ensure(L.total));
+    memcpy(ctx->hparams.p, sp.data(), n * sizeof(void *));
+    P2G_TRY(upload_params(ctx, L));
+    P2G_TRY(ctx->hash_out.ensure(round16(n * 16) + n * 4));
+    uint8_t *d_md5 = ctx->hash_out.as<uint8_t>();
+    uint32_t *d_crc = reinterpret_cast<uint32_t *>(d_md5 + round16(n * 16));
+    ctx->mark(1);
+    ctx->mark(2);
+    P2G_TRY(hash_run(ctx, reinterpret_cast<const uint8_t *const *>(ctx->params.p),
+                     static_cast<int>(n), S, d_md5, d_crc));
+    ctx->mark(3);
+    md5.resize(n * 16);
+    crc.resize(n);
+    P2G_CUDA(cudaMemcpyAsync(md5.data(), d_md5, n * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    P2G_CUDA(cudaMemcpyAsync(crc.data(), d_crc, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    return finish(ctx);
+}
+
+int p2g_hash_slices(p2g_ctx *ctx, const uint8_t *const *slices, size_t n, size_t slice_bytes,
+                    uint8_t *md5_out, uint32_t *crc_out, uint32_t flags)
+{
+    clear_error();
+    if (!ctx || (n && (!slices || !md5_out || !crc_out))) {
+        set_error("p2g_hash_slices: null argument");
+        return P2G_EINVAL;
+    }
+    if (n > 0x7fffffff) {
+        set_error("p2g_hash_slices: too many slices");
+        return P2G_ERANGE;
+    }
+    if (n == 0)
+        return P2G_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    begin(ctx);
+    std::vector<uint8_t> md5;
+    std::vector<uint32_t> crc;
+    P2G_TRY(hash_common(ctx, slices, n, slice_bytes, flags, md5, crc));
+    memcpy(md5_out, md5.data(), n * 16);
+    memcpy(crc_out, crc.data(), n * 4);
+    return P2G_OK;
+}
+
+int p2g_verify_slices(p2g_ctx *ctx, const uint8_t *const *slices, size_t n, size_t slice_bytes,
+                      const uint8_t *md5_expect, const uint32_t *crc_expect, uint8_t *ok_out,
+                      uint32_t flags)
+{
+    clear_error();
+    if (!ctx || (n && (!slices || !md5_expect || !crc_expect || !ok_out))) {
+        set_error("p2g_verify_slices: null argument");
+        return P2G_EINVAL;
+    }
+    if (n > 0x7fffffff) {
+        set_error("p2g_verify_slices: too many slices");
+        return P2G_ERANGE;
+    }
+    if (n == 0)
+        return P2G_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    begin(ctx);
+    std::vector<uint8_t> md5;
+    std::vector<uint32_t> crc;
+    P2G_TRY(hash_common(ctx, slices, n, slice_bytes, flags, md5, crc));
+    for (size_t i = 0; i < n; ++i)
+        ok_out[i] = crc[i] == crc_expect[i] && memcmp(&md5[i * 16], md5_expect + i * 16, 16) == 0;
+    return P2G_OK;
 }
 
 }  // extern "C"

@@ -52,6 +52,8 @@ struct p2g_ctx {
     // GF(2^16) log / antilog tables on the device (galois/core.rs:49-91)
     uint16_t *d_log = nullptr;
     uint16_t *d_exp = nullptr;
+    // CRC-32 slicing-by-4 tables on the device (4 x 256 words)
+    uint32_t *d_crc = nullptr;
     // scratch
     p2g::DevBuf planes;    // bit-sliced inputs
     p2g::DevBuf recs;      // coefficient records
@@ -65,6 +67,7 @@ struct p2g_ctx {
     p2g::DevBuf inv;       // decode matrix
     p2g::DevBuf gj_M;      // Gauss-Jordan augmented matrix
     p2g::DevBuf gj_status; // Gauss-Jordan status + pivots
+    p2g::DevBuf hash_out;  // MD5 + CRC results
 };
 
 #define P2G_CUDA(call)                                                                  \

@@ -17,8 +17,10 @@
 //   * Per input slice the CTA builds, in shared memory, two 256-row tables of
 //     every XOR combination of planes 0-7 and of planes 8-15 (64 KiB, lane L's
 //     column in bank L).  One output plane of one coefficient is then two
-//     conflict-free table reads and one XOR; the table rows to read are the
-//     coefficient's "record" (16 words), the same for all 32 lanes.
+//     table rows XORed; the rows to read are the coefficient's "record" (16
+//     words), the same for all 32 lanes.  ldmatrix.x4 serves as a 4-row
+//     gather: one instruction hands every lane its own word of four rows, so
+//     a coefficient costs 8 ldmatrix + 1 record load + 16 XORs per lane.
 //   * The next input's planes and records stream into a 4-slot shared-memory
 //     ring with cp.async while the current table is consumed; the table is
 //     double-buffered, one CTA barrier per input slice.
@@ -52,6 +54,16 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait()
 {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Four 8x8 b16 matrices from shared memory: lanes 8m..8m+7 give the row
+// addresses of matrix m, lane L receives word L % 4 of row L / 4 of each.
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t &d0, uint32_t &d1, uint32_t &d2,
+                                        uint32_t &d3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(d0), "=r"(d1), "=r"(d2), "=r"(d3)
+                 : "r"(addr));
 }
 
 // 32 little-endian u16 symbols at byte offset `off` of a 16-byte aligned
@@ -277,24 +289,27 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int j = 0; j < 16; ++j)
             acc[e][j] = 0;
 
+    // Lane L fetches, per plane pair, word L of four table rows with one
+    // ldmatrix.x4; it supplies the address of 16-byte chunk (L % 8) of the
+    // row of matrix L / 8 (record layout: bitslice.cuh make_record).
+    const uint32_t tab_s = static_cast<uint32_t>(__cvta_generic_to_shared(tab)) + (lane & 7) * 16;
     auto consume = [&](int i, int buf) {
         const uint4 *R = reinterpret_cast<const uint4 *>(ring + (i & (kRing - 1)) * SLOT +
                                                          kTileBytes) +
-                         my0 * 4;
-        const char *tb = reinterpret_cast<const char *>(tab + buf * kTableWords + lane);
+                         my0 * 4 + (lane >> 3);
+        const uint32_t tb = tab_s + buf * kTableBytes;
 #pragma unroll
         for (int e = 0; e < EREG; ++e) {
             if (e < myn) {
+                const uint4 r = R[e * 4];
+                const uint32_t w[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint4 r = R[e * 4 + q];
-                    const uint32_t w[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const uint32_t a = *reinterpret_cast<const uint32_t *>(tb + (w[k] & 0xFFFFu));
-                        const uint32_t b = *reinterpret_cast<const uint32_t *>(tb + (w[k] >> 16));
-                        acc[e][4 * q + k] ^= a ^ b;
-                    }
+                for (int p = 0; p < 8; ++p) {
+                    const uint32_t off = (p & 1) ? (w[p >> 1] >> 16) : (w[p >> 1] & 0xFFFFu);
+                    uint32_t d0, d1, d2, d3;
+                    ldsm_x4(tb + off, d0, d1, d2, d3);
+                    acc[e][2 * p] ^= d0 ^ d1;
+                    acc[e][2 * p + 1] ^= d2 ^ d3;
                 }
             }
         }

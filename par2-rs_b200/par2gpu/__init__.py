@@ -48,6 +48,11 @@ SIGNATURES = [
     ("p2g_muladd_region", _I, [_P, _P, _S, _P, _S, _P, _S, _S, _U32]),
     ("p2g_par2_constants", _I, [_S, _P]),
     ("p2g_encode", _I, [_P, _P, _S, _S, _P, _S, _P, _U32]),
+    ("p2g_invert", _I, [_P, _S, _P, _P]),
+    ("p2g_reconstruction_matrix", _I, [_P, _S, _P, _S, _P, _P]),
+    ("p2g_repair", _I, [_P, _S, _S, _P, _S, _P, _P, _P, _P, _U32]),
+    ("p2g_hash_slices", _I, [_P, _P, _S, _S, _P, _P, _U32]),
+    ("p2g_verify_slices", _I, [_P, _P, _S, _S, _P, _P, _P, _U32]),
 ]
 
 
@@ -193,3 +198,60 @@ class Context:
         out = np.zeros((len(exps), S), np.uint8)
         self.encode([src[i] for i in range(k)], S, exps, [out[e] for e in range(len(exps))])
         return out
+
+    # --- repair (par2_rs.rs:319-675) --------------------------------------
+    def invert(self, A):
+        """Exact GF(2^16) inverse of a square uint16 matrix (Par2GpuError with
+        code ESINGULAR when it has none)."""
+        A = np.ascontiguousarray(A, np.uint16)
+        out = np.zeros_like(A)
+        check(lib().p2g_invert(self.h, A.shape[0], A.ctypes.data, out.ctypes.data))
+        return out
+
+    def reconstruction_matrix(self, k, missing, exps):
+        miss = np.ascontiguousarray(missing, np.uint64)
+        e = np.ascontiguousarray(exps, np.uint32)
+        out = np.zeros((len(miss), len(miss)), np.uint16)
+        check(lib().p2g_reconstruction_matrix(self.h, k, miss.ctypes.data, len(miss),
+                                              e.ctypes.data, out.ctypes.data))
+        return out
+
+    def repair(self, k, slice_bytes, missing, present, exps, recovery, outs, device=False):
+        miss = np.ascontiguousarray(missing, np.uint64)
+        e = np.ascontiguousarray(exps, np.uint32)
+        check(lib().p2g_repair(self.h, k, slice_bytes, miss.ctypes.data, len(miss),
+                               _ptr_array(present), e.ctypes.data, _ptr_array(recovery),
+                               _ptr_array(outs), DEVICE_PTRS if device else 0))
+
+    def repair_array(self, data, missing, exps, recovery):
+        """Host convenience: data uint8 [k, S] (rows in `missing` ignored),
+        recovery uint8 [m, S] -> rebuilt slices uint8 [m, S]."""
+        data = np.ascontiguousarray(data, np.uint8)
+        k, S = data.shape
+        miss = sorted(int(x) for x in missing)
+        mset = set(miss)
+        present = [data[i] for i in range(k) if i not in mset]
+        rec = np.ascontiguousarray(recovery, np.uint8)
+        out = np.zeros((len(miss), S), np.uint8)
+        self.repair(k, S, miss, present, exps, [rec[j] for j in range(len(miss))],
+                    [out[j] for j in range(len(miss))])
+        return out
+
+    # --- per-slice MD5 + CRC32 (verify.rs:548-654, creator.rs:397-409) ----
+    def hash_slices(self, slices, slice_bytes, device=False):
+        n = len(slices)
+        md5 = np.zeros((n, 16), np.uint8)
+        crc = np.zeros(n, np.uint32)
+        check(lib().p2g_hash_slices(self.h, _ptr_array(slices), n, slice_bytes, md5.ctypes.data,
+                                    crc.ctypes.data, DEVICE_PTRS if device else 0))
+        return md5, crc
+
+    def verify_slices(self, slices, slice_bytes, md5_expect, crc_expect, device=False):
+        n = len(slices)
+        md5e = np.ascontiguousarray(md5_expect, np.uint8).reshape(n, 16)
+        crce = np.ascontiguousarray(crc_expect, np.uint32)
+        ok = np.zeros(n, np.uint8)
+        check(lib().p2g_verify_slices(self.h, _ptr_array(slices), n, slice_bytes,
+                                      md5e.ctypes.data, crce.ctypes.data, ok.ctypes.data,
+                                      DEVICE_PTRS if device else 0))
+        return ok.astype(bool)

@@ -1,0 +1,156 @@
+"""GPU parity of the repair path: device Gauss-Jordan (K2) and the two
+multiply-accumulate passes, through the C ABI, against the oracle and the
+QuickPar fixture (par2-rs tests/external_multiblock_repair.rs:50-247)."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests import quickpar
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import par2gpu
+
+    c = par2gpu.Context(0)
+    yield c
+    c.close()
+
+
+def par2_matrix(k, missing, exps):
+    c = oracle.par2_constants(k)
+    return np.array([[oracle.gf_pow(int(c[j]), int(e)) for j in missing] for e in exps], np.uint16)
+
+
+@pytest.mark.parametrize("m", [1, 2, 13, 64, 200])
+def test_reconstruction_matrix_matches_oracle(ctx, m):
+    rng = np.random.default_rng(m)
+    k = 4 * m + 7
+    missing = np.sort(rng.choice(k, m, replace=False))
+    exps = np.arange(m)
+    got = ctx.reconstruction_matrix(k, missing, exps)
+    want = oracle.invert(par2_matrix(k, missing, exps))
+    assert want is not None
+    assert np.array_equal(got, want)
+
+
+def test_invert_random_and_singular(ctx):
+    import par2gpu
+
+    rng = np.random.default_rng(9)
+    for m in (3, 17, 50):
+        A = rng.integers(0, 65536, (m, m), dtype=np.uint16)
+        want = oracle.invert(A)
+        if want is None:
+            continue
+        assert np.array_equal(ctx.invert(A), want)
+    # zero diagonal entries force the reference's row swap
+    A = np.array([[0, 1, 2], [3, 0, 5], [7, 11, 0]], np.uint16)
+    assert np.array_equal(ctx.invert(A), oracle.invert(A))
+    S = np.array([[1, 2, 3], [2, 4, 6], [5, 6, 7]], np.uint16)
+    S[1] = [oracle.gf_mul(2, int(v)) for v in S[0]]
+    assert oracle.invert(S) is None
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        ctx.invert(S)
+    assert ei.value.code == par2gpu.ESINGULAR
+    assert "Singular matrix" in par2gpu.last_error()
+
+
+def test_quickpar_repair_scenarios(ctx):
+    qp = quickpar.load()
+    src, _ = qp.slices()
+    bs = qp.block_size
+    t1 = qp.slice_base("test-1.data")
+    t4 = qp.slice_base("test-4.data")
+    n1 = (len(qp.files[qp.file_index("test-1.data")]["data"]) + bs - 1) // bs
+    cases = {"single": [t1], "two_in_one": [t1, t1 + 3], "three_in_one": [t1, t1 + 2, t1 + 5],
+             "two_files": [t1 + 1, t4 + 2], "deleted_file": list(range(t1, t1 + n1))}
+    for name, dmg in cases.items():
+        m = len(dmg)
+        data = src.copy()
+        data[dmg] = 0xAB
+        rec = np.stack([qp.recovery[e] for e in range(m)])
+        got = ctx.repair_array(data, dmg, np.arange(m), rec)
+        assert np.array_equal(got, src[dmg]), name
+
+
+@pytest.mark.parametrize("k,S,m", [(40, 4096, 1), (40, 4098, 5), (256, 8192, 13), (120, 6144, 60)])
+def test_repair_matches_oracle(ctx, k, S, m):
+    rng = np.random.default_rng(k + m)
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(m, dtype=np.uint32)
+    rec = ctx.encode_array(src, exps)
+    missing = np.sort(rng.choice(k, m, replace=False))
+    data = src.copy()
+    data[missing] = 0
+    want, moved = oracle.reconstruct(data, missing, exps, rec)
+    got = ctx.repair_array(data, missing, exps, rec)
+    assert np.array_equal(got, want)
+    assert np.array_equal(got, src[missing])
+
+
+def test_repair_with_sparse_exponents(ctx):
+    rng = np.random.default_rng(77)
+    k, S = 64, 4096
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    all_exps = np.arange(20, dtype=np.uint32)
+    rec = ctx.encode_array(src, all_exps)
+    # recovery slices 0, 2, 3 were lost: the lowest surviving exponents are used
+    avail = [e for e in range(20) if e not in (0, 2, 3)]
+    missing = np.sort(rng.choice(k, 6, replace=False))
+    use = np.array(avail[:6], np.uint32)
+    data = src.copy()
+    data[missing] = 0
+    got = ctx.repair_array(data, missing, use, rec[use])
+    want, _ = oracle.reconstruct(data, missing, use, rec[use])
+    assert np.array_equal(got, want)
+    assert np.array_equal(got, src[missing])
+
+
+def test_plain_config_roundtrip(ctx):
+    """16 MiB file, 64 KiB slices: k=256, r=13; zero 13 random slices and
+    repair (the CPU-runnable plain configuration)."""
+    rng = np.random.default_rng(2026)
+    k, S, r = 256, 65536, 13
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(r, dtype=np.uint32)
+    rec = ctx.encode_array(src, exps)
+    assert np.array_equal(rec, oracle.encode(src, exps))
+    missing = np.sort(rng.choice(k, r, replace=False))
+    data = src.copy()
+    data[missing] = 0
+    got = ctx.repair_array(data, missing, exps, rec)
+    want, _ = oracle.reconstruct(data, missing, exps, rec)
+    assert np.array_equal(got, want)
+    assert np.array_equal(got, src[missing])
+
+
+def test_repair_device_pointers(ctx):
+    import torch
+
+    rng = np.random.default_rng(5)
+    k, S, m = 50, 8192, 7
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(m, dtype=np.uint32)
+    rec = ctx.encode_array(src, exps)
+    missing = np.sort(rng.choice(k, m, replace=False))
+    d_src = torch.from_numpy(src).cuda()
+    d_rec = torch.from_numpy(rec).cuda()
+    d_out = torch.zeros((m, S), dtype=torch.uint8, device="cuda")
+    mset = set(missing.tolist())
+    present = [d_src[i] for i in range(k) if i not in mset]
+    ctx.repair(k, S, missing, present, exps, [d_rec[j] for j in range(m)],
+               [d_out[j] for j in range(m)], device=True)
+    assert np.array_equal(d_out.cpu().numpy(), src[missing])
+
+
+def test_repair_argument_errors(ctx):
+    import par2gpu
+
+    data = np.zeros((4, 8), np.uint8)
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        ctx.repair(4, 8, [2, 1], [data[0], data[3]], [0, 1], [data[0], data[0]],
+                   [data[1], data[2]])
+    assert ei.value.code == par2gpu.EINVAL
