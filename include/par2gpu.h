@@ -155,6 +155,32 @@ int p2g_verify_slices(p2g_ctx *ctx, const uint8_t *const *slices, size_t n, size
                       const uint8_t *md5_expect, const uint32_t *crc_expect, uint8_t *ok_out,
                       uint32_t flags);
 
+/* Size of the fixed device scratch array behind p2g_encode_noalloc. */
+#define P2G_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* Recovery-slice creation (the work of p2g_encode) for callers that cannot
+ * allocate device memory at call time: services that reserved a fixed
+ * device-memory budget up front, latency paths that cannot take cudaMalloc's
+ * implicit synchronisation, hosts that forbid allocation after start-up.  No
+ * counterpart in par2-rs.
+ *   - Allocates nothing: its scratch is one static device array of
+ *     P2G_NOALLOC_SCRATCH_BYTES on every GPU that loads this library, held
+ *     until the process exits.  A problem whose scratch (about k*r*66 bytes
+ *     plus k*slice_bytes rounded up to 2 KiB tiles plus the pointer tables)
+ *     exceeds it returns P2G_ERANGE.
+ *   - src[k] / out[r] are 16-byte aligned DEVICE pointers on the current
+ *     device; the pointer arrays and exps are host arrays.
+ *   - The work is enqueued on cuda_stream (a cudaStream_t; NULL is the legacy
+ *     default stream) and the call returns without waiting for it;
+ *     synchronise the stream before reading the outputs.
+ *   - The first call on a device sets that device up (it looks up the device
+ *     address of the scratch array, which loads the module); make that first
+ *     call before any stream capture.
+ *   - All calls on a device share the array: calls whose work overlaps on the
+ *     GPU race, and the caller must serialise them. */
+int p2g_encode_noalloc(void *cuda_stream, const uint8_t *const *src, size_t k,
+                       size_t slice_bytes, const uint32_t *exps, size_t r, uint8_t *const *out);
+
 #ifdef __cplusplus
 }
 #endif

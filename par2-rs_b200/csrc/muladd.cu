@@ -491,4 +491,53 @@ int muladd_run(p2g_ctx *ctx, const uint8_t *const *d_src, int nin, uint8_t *cons
     return P2G_OK;
 }
 
+size_t planes_bytes_fixed(int nin, size_t S)
+{
+    return static_cast<size_t>(nin) * ((S + kTileBytes - 1) / kTileBytes) * kTileBytes;
+}
+
+int records_matrix_fixed(cudaStream_t stream, const uint16_t *d_coeff, int nin, int nout,
+                         uint32_t *d_recs)
+{
+    size_t n = static_cast<size_t>(nin) * nout;
+    if (n == 0)
+        return P2G_OK;
+    records_matrix_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(
+        d_coeff, nin, nout, d_recs);
+    P2G_CUDA(cudaGetLastError());
+    return P2G_OK;
+}
+
+int muladd_run_fixed(cudaStream_t stream, int sm_count, const uint8_t *const *d_src, int nin,
+                     uint8_t *const *d_dst, int nout, size_t S, const uint32_t *d_recs,
+                     uint32_t *d_planes)
+{
+    if (nout <= 0)
+        return P2G_OK;
+    p2g_ctx probe;  // choose_plan reads only sm_count
+    probe.sm_count = sm_count;
+    const MuladdPlan p = choose_plan(&probe, nin, nout, S);
+    const int T = static_cast<int>((S + kTileBytes - 1) / kTileBytes);
+    dim3 zg(static_cast<unsigned>(std::min<size_t>((S + 4095) / 4096, 1024)), nout);
+    if (nin == 0 || p.nsplit > 1) {
+        zero_slices<<<zg, 256, 0, stream>>>(d_dst, nout, S);
+        P2G_CUDA(cudaGetLastError());
+        if (nin == 0)
+            return P2G_OK;
+    }
+    size_t groups = static_cast<size_t>(nin) * T * 32;
+    slices_to_planes<<<static_cast<unsigned>((groups + 255) / 256), 256, 0, stream>>>(
+        d_src, nin, T, S, d_planes);
+    P2G_CUDA(cudaGetLastError());
+    KernelFn fn = kernel_for(p.ereg);
+    size_t smem = smem_bytes(p.ereg);
+    P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    long long grid = static_cast<long long>(T) * p.nblk * p.nsplit;
+    fn<<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(
+        d_planes, d_recs, nin, nout, T, p.nblk, p.nsplit, d_dst, S, 0);
+    P2G_CUDA(cudaGetLastError());
+    return P2G_OK;
+}
+
 }  // namespace p2g

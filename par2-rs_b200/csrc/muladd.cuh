@@ -31,4 +31,14 @@ int muladd_run(p2g_ctx *ctx, const uint8_t *const *d_src, int nin, uint8_t *cons
                int nout, size_t slice_bytes, const uint32_t *d_recs, int mode,
                const MuladdPlan *plan = nullptr);
 
+// The same work as records_from_matrix / muladd_run (store mode) on a given
+// stream with caller-provided scratch: nothing is allocated.  d_planes must
+// hold planes_bytes_fixed(nin, S) bytes.
+size_t planes_bytes_fixed(int nin, size_t S);
+int records_matrix_fixed(cudaStream_t stream, const uint16_t *d_coeff, int nin, int nout,
+                         uint32_t *d_recs);
+int muladd_run_fixed(cudaStream_t stream, int sm_count, const uint8_t *const *d_src, int nin,
+                     uint8_t *const *d_dst, int nout, size_t S, const uint32_t *d_recs,
+                     uint32_t *d_planes);
+
 }  // namespace p2g

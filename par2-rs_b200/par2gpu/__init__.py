@@ -53,7 +53,9 @@ SIGNATURES = [
     ("p2g_repair", _I, [_P, _S, _S, _P, _S, _P, _P, _P, _P, _U32]),
     ("p2g_hash_slices", _I, [_P, _P, _S, _S, _P, _P, _U32]),
     ("p2g_verify_slices", _I, [_P, _P, _S, _S, _P, _P, _P, _U32]),
+    ("p2g_encode_noalloc", _I, [_P, _P, _S, _S, _P, _S, _P]),
 ]
+NOALLOC_SCRATCH_BYTES = 64 << 20
 
 
 class Timing(ctypes.Structure):
@@ -111,6 +113,15 @@ def par2_constants(k):
     out = np.zeros(k, np.uint16)
     check(lib().p2g_par2_constants(k, out.ctypes.data))
     return out
+
+
+def encode_noalloc(stream, srcs, slice_bytes, exps, outs):
+    """p2g_encode_noalloc: encode into caller device buffers with the library's
+    fixed static scratch only (for callers that cannot allocate); enqueued on
+    `stream` (an int cudaStream_t handle, 0 = default stream), not waited for."""
+    e = np.ascontiguousarray(exps, np.uint32)
+    check(lib().p2g_encode_noalloc(stream or None, _ptr_array(srcs), len(srcs), slice_bytes,
+                                   e.ctypes.data, len(e), _ptr_array(outs)))
 
 
 def _ptr(x):
