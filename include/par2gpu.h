@@ -72,7 +72,7 @@ int p2g_set_stream(p2g_ctx *ctx, void *cuda_stream);
 typedef struct {
     float ms_records;  /* coefficient records */
     float ms_planes;   /* slices -> bit planes */
-    float ms_muladd;   /* the multiply-accumulate kernel */
+    float ms_kernel;   /* the main kernel: multiply-accumulate, or hashing */
     float ms_total;    /* first to last event of the call */
     int launches;      /* kernels launched by the call */
 } p2g_timing;

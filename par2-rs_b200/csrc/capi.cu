@@ -188,7 +188,7 @@ static int finish(p2g_ctx *ctx)
     if (ctx->timing) {
         ctx->last.ms_records = elapsed(ctx, 0, 1);
         ctx->last.ms_planes = elapsed(ctx, 1, 2);
-        ctx->last.ms_muladd = elapsed(ctx, 2, 3);
+        ctx->last.ms_kernel = elapsed(ctx, 2, 3);
         ctx->last.ms_total = elapsed(ctx, 0, 4);
     }
     return P2G_OK;

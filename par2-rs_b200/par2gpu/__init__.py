@@ -61,7 +61,7 @@ NOALLOC_SCRATCH_BYTES = 64 << 20
 class Timing(ctypes.Structure):
     """p2g_timing: per-phase device milliseconds of the last call."""
     _fields_ = [("ms_records", ctypes.c_float), ("ms_planes", ctypes.c_float),
-                ("ms_muladd", ctypes.c_float), ("ms_total", ctypes.c_float),
+                ("ms_kernel", ctypes.c_float), ("ms_total", ctypes.c_float),
                 ("launches", ctypes.c_int)]
 
 
