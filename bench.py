@@ -208,6 +208,10 @@ def run_ours(args, rank, world):
     def step_dev():
         ctx.encode(src_ptrs, S, exps, out_ptrs, device=True)
 
+    plan = None
+    if not args.no_autotune:
+        plan = ctx.autotune(k, r, S).as_dict()
+
     def barrier():
         if world > 1:
             dist.barrier()
@@ -247,7 +251,8 @@ def run_ours(args, rank, world):
     if args.quick:
         ctx.close()
         if rank == 0:
-            print(json.dumps({"workload": WORKLOAD, "ms_per_step": ms_step, "value": value,
+            print(json.dumps({"workload": WORKLOAD, "plan": plan, "ms_per_step": ms_step,
+                              "value": value,
                               "unit": "GB/s", "kernel_ms": sum(mul_ms) / len(mul_ms),
                               "gpu_launches": launches, "clocks": clk}), flush=True)
         return
@@ -314,6 +319,7 @@ def run_ours(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u16 (GF(2^16))", "data": "synthetic (seeded uniform bytes)",
             "config": {"workload": WORKLOAD, "k": k, "r": r, "slice_bytes": S,
+                       "plan": plan if plan else "heuristic",
                        "parallelism": f"{world} independent sets" if world > 1 else "1 set",
                        "l2": "inputs 2 GiB per step > 126 MB L2; no flush"},
             "roofline": roofline,
@@ -418,6 +424,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large_encode",
                     choices=sorted(WORKLOADS) + ["verify_repair"])
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the heuristic tile shape instead of the autotuned one")
     ap.add_argument("--quick", action="store_true",
                     help="device-resident timing only (no e2e, roofline probe or CPU baseline)")
     args = ap.parse_args()

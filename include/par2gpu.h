@@ -79,6 +79,35 @@ typedef struct {
 int p2g_set_timing(p2g_ctx *ctx, int enable);
 int p2g_last_timing(p2g_ctx *ctx, p2g_timing *out);
 
+/* Tile shape of the multiply-accumulate kernel for one problem shape:
+ * warps per CTA; warps_per_group warps share one group of outputs_per_group
+ * outputs (each holding 16 / warps_per_group of the 16 bit planes); output
+ * blocks of (warps / warps_per_group) * outputs_per_group outputs; input
+ * splits (partial sums folded with atomic XOR); and the kernel time it
+ * measured at (ms, set by p2g_autotune).  No counterpart in par2-rs, whose
+ * strategies fix their blocking (avx2.rs:700-701 DEST_BATCH / SRC_BATCH). */
+typedef struct {
+    int warps;
+    int outputs_per_group;
+    int warps_per_group;
+    int output_blocks;
+    int input_splits;
+    float ms;
+} p2g_plan;
+
+/* Autotuner: times every compiled tile shape (and output-block / input-split
+ * choice) of the multiply-accumulate kernel for nin inputs x nout outputs of
+ * slice_bytes on synthetic data in the context's scratch (best of `reps`
+ * launches each) and makes the fastest the context's plan for that shape.
+ * Untuned shapes use a heuristic plan. */
+int p2g_autotune(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes, int reps,
+                 p2g_plan *best);
+
+/* Pins the plan for one shape (P2G_EINVAL if the shape is not compiled or
+ * does not cover nout outputs). */
+int p2g_set_plan(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes,
+                 const p2g_plan *plan);
+
 /* GaloisSimdStrategy::{name, is_available, priority}
  * (galois/simd/mod.rs:26-33): "CUDA-sm100a", available iff an sm_100 device
  * is present, priority P2G_PRIORITY_OPTIMAL. */

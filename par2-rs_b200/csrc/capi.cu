@@ -394,6 +394,55 @@ int p2g_last_timing(p2g_ctx *ctx, p2g_timing *out)
     return P2G_OK;
 }
 
+int p2g_autotune(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes, int reps,
+                 p2g_plan *best)
+{
+    clear_error();
+    if (!ctx || !best) {
+        set_error("p2g_autotune: null argument");
+        return P2G_EINVAL;
+    }
+    if (nin > 65535 || nout > 65535) {
+        set_error("p2g_autotune: %zu x %zu beyond 65535", nin, nout);
+        return P2G_ERANGE;
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    MuladdPlan p;
+    float ms = 0.f;
+    int tried = 0;
+    P2G_TRY(muladd_autotune(ctx, static_cast<int>(nin), static_cast<int>(nout), slice_bytes,
+                            reps, &p, &ms, &tried));
+    *best = p2g_plan{p.warps, p.ereg, p.psplit, p.nblk, p.nsplit, ms};
+    return P2G_OK;
+}
+
+int p2g_set_plan(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes,
+                 const p2g_plan *plan)
+{
+    clear_error();
+    if (!ctx || !plan) {
+        set_error("p2g_set_plan: null argument");
+        return P2G_EINVAL;
+    }
+    MuladdPlan p;
+    p.warps = plan->warps;
+    p.ereg = plan->outputs_per_group;
+    p.psplit = plan->warps_per_group;
+    p.nblk = plan->output_blocks;
+    p.nsplit = plan->input_splits;
+    if (nin > 65535 || nout > 65535 ||
+        !plan_valid(p, static_cast<int>(nin), static_cast<int>(nout), slice_bytes)) {
+        set_error("p2g_set_plan: warps=%d outputs_per_group=%d warps_per_group=%d blocks=%d "
+                  "splits=%d is not a compiled shape covering %zu outputs",
+                  p.warps, p.ereg, p.psplit, p.nblk, p.nsplit, nout);
+        return P2G_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->plans[plan_key(static_cast<int>(nin), static_cast<int>(nout), slice_bytes)] = p;
+    return P2G_OK;
+}
+
 int p2g_par2_constants(size_t k, uint16_t *out)
 {
     clear_error();

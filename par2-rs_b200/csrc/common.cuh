@@ -4,8 +4,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 
 #include "../../include/par2gpu.h"
 
@@ -26,9 +28,26 @@ struct DevBuf {
     T *as() const { return static_cast<T *>(p); }
 };
 
+// How one multiply-accumulate problem is cut into CTAs: warps per CTA,
+// outputs per output group (16 / psplit accumulator registers per warp each),
+// output blocks of (warps / psplit) * ereg outputs, input ranges folded with
+// atomic XOR.
+struct MuladdPlan {
+    int warps = 8;
+    int ereg = 1;
+    int nblk = 1;
+    int nsplit = 1;
+    int psplit = 1;  // warps sharing one output group (each holds 16/psplit planes)
+};
+
+using PlanKey = std::tuple<int, int, size_t>;  // inputs, outputs, slice bytes
+inline PlanKey plan_key(int nin, int nout, size_t S) { return PlanKey(nin, nout, S); }
+
 }  // namespace p2g
 
 struct p2g_ctx {
+    // tuned plans (p2g_autotune); choose_plan falls back to a heuristic
+    std::map<p2g::PlanKey, p2g::MuladdPlan> plans;
     int device = 0;
     int sm_count = 0;
     cudaStream_t own_stream = nullptr;  // created with the context

@@ -27,19 +27,17 @@
 //   * Few tiles / outputs: the input range is split across CTAs and the
 //     partial sums are folded into the output with atomic XOR.
 #include <algorithm>
+#include <vector>
 
 #include "bitslice.cuh"
 #include "muladd.cuh"
 
 namespace p2g {
 
-constexpr int kWarps = 8;
-constexpr int kThreads = kWarps * 32;
 constexpr int kTileBytes = 2048;             // 1024 symbols
 constexpr int kTableWords = 512 * 32;        // T0 and T1, 128 B per row
 constexpr int kTableBytes = kTableWords * 4; // 64 KiB
 constexpr int kRing = 4;
-constexpr int kMaxEreg = 13;
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
@@ -208,13 +206,19 @@ __global__ void records_par2_kernel(const uint16_t *__restrict__ consts,
     put_record(recs, gid, c);
 }
 
-template <int EREG>
-__global__ void __launch_bounds__(kThreads, 1)
+// WARPS warps per CTA; each output group of EREG outputs is held by PSPLIT
+// warps, each keeping 16 / PSPLIT of the 16 planes (PSPLIT = 2 doubles the
+// warps per SM at the same number of outputs per table).
+template <int WARPS, int EREG, int PSPLIT>
+__global__ void __launch_bounds__(WARPS * 32, 1)
     muladd_bitsliced(const uint32_t *__restrict__ planes, const uint32_t *__restrict__ recs,
                      int nin, int nout, int T, int nblk, int nsplit,
                      uint8_t *const *__restrict__ dst, size_t S, int mode)
 {
-    constexpr int EBLK = kWarps * EREG;
+    constexpr int THREADS = WARPS * 32;
+    constexpr int GROUPS = WARPS / PSPLIT;   // output groups
+    constexpr int NPL = 16 / PSPLIT;         // planes per warp
+    constexpr int EBLK = GROUPS * EREG;
     constexpr int SLOT = kTileBytes + EBLK * 64;
     extern __shared__ __align__(128) uint8_t smem[];
     uint32_t *tab = reinterpret_cast<uint32_t *>(smem);
@@ -231,7 +235,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int nb = min(EBLK, nout - obase);
     const int i0 = static_cast<int>(static_cast<long long>(nin) * split / nsplit);
     const int i1 = static_cast<int>(static_cast<long long>(nin) * (split + 1) / nsplit);
-    const int my0 = warp * EREG;
+    const int ph = warp % PSPLIT;            // which planes: [ph*NPL, ph*NPL + NPL)
+    const int my0 = (warp / PSPLIT) * EREG;
     const int myn = max(0, min(EREG, nb - my0));
 
     auto issue = [&](int i) {
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint8_t *gr = reinterpret_cast<const uint8_t *>(
                 recs + (static_cast<size_t>(i) * nout + obase) * 16);
             const int nchunk = 128 + nb * 4;
-            for (int c = threadIdx.x; c < nchunk; c += kThreads) {
+            for (int c = threadIdx.x; c < nchunk; c += THREADS) {
                 if (c < 128)
                     cp_async16(s + c * 16, gp + c * 16);
                 else
@@ -252,10 +257,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         cp_async_commit();
     };
 
-    // Table rows [64*wq, 64*wq+64) of half `half` (planes 8*half .. 8*half+7).
+    // The 512 table rows form 32 groups of 16 (half = g / 16 selects planes
+    // 0-7 or 8-15; h = g % 16 is the pattern of the half's planes 4-7, the
+    // row's low nibble the pattern of its planes 0-3).  Warp w builds groups
+    // [32w/WARPS, 32(w+1)/WARPS), which never straddle the two halves for
+    // WARPS in {8, 12, 16}.
     auto build = [&](int i, int buf) {
         const uint32_t *P = reinterpret_cast<const uint32_t *>(ring + (i & (kRing - 1)) * SLOT);
-        const int half = warp >> 2, wq = warp & 3;
+        const int g0 = warp * 32 / WARPS, g1 = (warp + 1) * 32 / WARPS;
+        const int half = g0 >> 4;
         uint32_t p[8];
 #pragma unroll
         for (int b = 0; b < 8; ++b)
@@ -272,21 +282,27 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int x = 0; x < 8; ++x)
             L[8 + x] = L[x] ^ p[3];
-        uint32_t base = ((wq & 1) ? p[6] : 0u) ^ ((wq & 2) ? p[7] : 0u);
-        uint32_t H[4] = {base, base ^ p[4], base ^ p[5], base ^ p[4] ^ p[5]};
-        uint32_t *T0 = tab + buf * kTableWords + (half * 256 + wq * 64) * 32 + lane;
+        constexpr int GMAX = (32 + WARPS - 1) / WARPS;
+        const int h0 = g0 & 15;
+        uint32_t *T0 = tab + buf * kTableWords + (half * 256 + h0 * 16) * 32 + lane;
 #pragma unroll
-        for (int hh = 0; hh < 4; ++hh)
+        for (int gg = 0; gg < GMAX; ++gg) {
+            if (GMAX * WARPS == 32 || g0 + gg < g1) {
+                const int h = h0 + gg;
+                const uint32_t H = ((h & 1) ? p[4] : 0u) ^ ((h & 2) ? p[5] : 0u) ^
+                                   ((h & 4) ? p[6] : 0u) ^ ((h & 8) ? p[7] : 0u);
 #pragma unroll
-            for (int x = 0; x < 16; ++x)
-                T0[(hh * 16 + x) * 32] = H[hh] ^ L[x];
+                for (int x = 0; x < 16; ++x)
+                    T0[(gg * 16 + x) * 32] = H ^ L[x];
+            }
+        }
     };
 
-    uint32_t acc[EREG][16];
+    uint32_t acc[EREG][NPL];
 #pragma unroll
     for (int e = 0; e < EREG; ++e)
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
+        for (int j = 0; j < NPL; ++j)
             acc[e][j] = 0;
 
     // Lane L fetches, per plane pair, word L of four table rows with one
@@ -301,10 +317,21 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int e = 0; e < EREG; ++e) {
             if (e < myn) {
-                const uint4 r = R[e * 4];
-                const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+                uint32_t w[4];
+                if constexpr (PSPLIT == 1) {
+                    const uint4 r = R[e * 4];
+                    w[0] = r.x;
+                    w[1] = r.y;
+                    w[2] = r.z;
+                    w[3] = r.w;
+                } else {
+                    // plane pairs [4ph, 4ph+4): record words 2ph, 2ph+1
+                    const uint2 r = reinterpret_cast<const uint2 *>(R + e * 4)[ph];
+                    w[0] = r.x;
+                    w[1] = r.y;
+                }
 #pragma unroll
-                for (int p = 0; p < 8; ++p) {
+                for (int p = 0; p < NPL / 2; ++p) {
                     const uint32_t off = (p & 1) ? (w[p >> 1] >> 16) : (w[p >> 1] & 0xFFFFu);
                     uint32_t d0, d1, d2, d3;
                     ldsm_x4(tb + off, d0, d1, d2, d3);
@@ -335,16 +362,42 @@ __global__ void __launch_bounds__(kThreads, 1)
     cp_async_wait<0>();
 
     const int smode = nsplit > 1 ? 2 : mode;
+    if constexpr (PSPLIT == 1) {
 #pragma unroll
-    for (int e = 0; e < EREG; ++e) {
-        if (e < myn) {
-            uint32_t x[16];
+        for (int e = 0; e < EREG; ++e) {
+            if (e < myn) {
+                uint32_t x[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
-                x[j] = acc[e][j];
-            transpose16x2(x);
-            store_group(dst[obase + my0 + e], S, static_cast<size_t>(t) * kTileBytes + lane * 64,
-                        x, smode);
+                for (int j = 0; j < 16; ++j)
+                    x[j] = acc[e][j];
+                transpose16x2(x);
+                store_group(dst[obase + my0 + e], S,
+                            static_cast<size_t>(t) * kTileBytes + lane * 64, x, smode);
+            }
+        }
+    } else {
+        // the odd warp of each pair hands its planes 8-15 to the even warp
+        // through shared memory (the tables are no longer needed)
+        uint32_t *xch = tab + (warp / 2) * (8 * 32);
+#pragma unroll
+        for (int e = 0; e < EREG; ++e) {
+            __syncthreads();
+            if (ph == 1 && e < myn)
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    xch[j * 32 + lane] = acc[e][j];
+            __syncthreads();
+            if (ph == 0 && e < myn) {
+                uint32_t x[16];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    x[j] = acc[e][j];
+                    x[8 + j] = xch[j * 32 + lane];
+                }
+                transpose16x2(x);
+                store_group(dst[obase + my0 + e], S,
+                            static_cast<size_t>(t) * kTileBytes + lane * 64, x, smode);
+            }
         }
     }
 }
@@ -369,38 +422,67 @@ __global__ void zero_slices(uint8_t *const *__restrict__ dst, int nout, size_t S
 using KernelFn = void (*)(const uint32_t *, const uint32_t *, int, int, int, int, int,
                           uint8_t *const *, size_t, int);
 
-static KernelFn kernel_for(int ereg)
+struct Variant {
+    int warps, ereg, psplit;
+    KernelFn fn;
+};
+
+// Compiled tile shapes: warps per CTA x outputs per warp.  The register
+// budget (64K per SM, one CTA per SM) caps EREG at 13 / 8 / 5 for 8 / 12 / 16
+// warps without spills.
+#define P2G_V(W, E, P) {W, E, P, muladd_bitsliced<W, E, P>}
+static const Variant kVariants[] = {
+    P2G_V(8, 1, 1),   P2G_V(8, 2, 1),   P2G_V(8, 3, 1),   P2G_V(8, 4, 1),   P2G_V(8, 5, 1),
+    P2G_V(8, 6, 1),   P2G_V(8, 7, 1),   P2G_V(8, 8, 1),   P2G_V(8, 9, 1),   P2G_V(8, 10, 1),
+    P2G_V(8, 11, 1),  P2G_V(8, 12, 1),  P2G_V(8, 13, 1),  P2G_V(12, 4, 1),  P2G_V(12, 6, 1),
+    P2G_V(12, 7, 1),  P2G_V(12, 8, 1),  P2G_V(16, 2, 1),  P2G_V(16, 3, 1),  P2G_V(16, 4, 1),
+    P2G_V(16, 5, 1),  P2G_V(16, 8, 2),  P2G_V(16, 10, 2), P2G_V(16, 12, 2), P2G_V(16, 13, 2),
+};
+#undef P2G_V
+
+static KernelFn kernel_for(int warps, int ereg, int psplit)
 {
-    switch (ereg) {
-    case 1: return muladd_bitsliced<1>;
-    case 2: return muladd_bitsliced<2>;
-    case 3: return muladd_bitsliced<3>;
-    case 4: return muladd_bitsliced<4>;
-    case 5: return muladd_bitsliced<5>;
-    case 6: return muladd_bitsliced<6>;
-    case 7: return muladd_bitsliced<7>;
-    case 8: return muladd_bitsliced<8>;
-    case 9: return muladd_bitsliced<9>;
-    case 10: return muladd_bitsliced<10>;
-    case 11: return muladd_bitsliced<11>;
-    case 12: return muladd_bitsliced<12>;
-    case 13: return muladd_bitsliced<13>;
-    default: return nullptr;
-    }
+    for (const Variant &v : kVariants)
+        if (v.warps == warps && v.ereg == ereg && v.psplit == psplit)
+            return v.fn;
+    return nullptr;
 }
 
-static size_t smem_bytes(int ereg)
+int muladd_variants(int *warps, int *eregs, int *psplits, int cap)
 {
-    return 2 * kTableBytes + kRing * (kTileBytes + kWarps * ereg * 64);
+    int n = 0;
+    for (const Variant &v : kVariants) {
+        if (n < cap) {
+            warps[n] = v.warps;
+            eregs[n] = v.ereg;
+            psplits[n] = v.psplit;
+        }
+        ++n;
+    }
+    return n;
+}
+
+// outputs one CTA of this shape covers
+static int block_outputs(const MuladdPlan &p) { return p.warps / p.psplit * p.ereg; }
+
+static size_t smem_bytes(const MuladdPlan &p)
+{
+    return 2 * kTableBytes + kRing * (kTileBytes + block_outputs(p) * 64);
 }
 
 MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t S)
 {
+    if (ctx) {
+        auto it = ctx->plans.find(plan_key(nin, nout, S));
+        if (it != ctx->plans.end())
+            return it->second;
+    }
     MuladdPlan p;
     const int T = static_cast<int>((S + kTileBytes - 1) / kTileBytes);
-    p.nblk = (nout + kWarps * kMaxEreg - 1) / (kWarps * kMaxEreg);
-    p.ereg = (nout + kWarps * p.nblk - 1) / (kWarps * p.nblk);
-    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    p.warps = 8;
+    p.nblk = (nout + 8 * 13 - 1) / (8 * 13);
+    p.ereg = (nout + 8 * p.nblk - 1) / (8 * p.nblk);
+    const int sms = ctx && ctx->sm_count > 0 ? ctx->sm_count : 148;
     const long long ctas = static_cast<long long>(T) * p.nblk;
     // The atomic-XOR fold touches whole aligned words: only for S % 4 == 0.
     if (ctas < 2LL * sms && S % 4 == 0) {
@@ -409,6 +491,15 @@ MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t S)
         p.nsplit = static_cast<int>(std::min(want, cap));
     }
     return p;
+}
+
+bool plan_valid(const MuladdPlan &p, int nin, int nout, size_t S)
+{
+    if (p.psplit < 1 || kernel_for(p.warps, p.ereg, p.psplit) == nullptr || p.nblk < 1)
+        return false;
+    const long long eb = block_outputs(p);
+    return p.nblk * eb >= nout && (p.nblk - 1) * eb < nout && p.nsplit >= 1 &&
+           (p.nsplit == 1 || (S % 4 == 0 && p.nsplit <= std::max(1, nin)));
 }
 
 int records_from_matrix(p2g_ctx *ctx, const uint16_t *d_coeff, int nin, int nout,
@@ -437,6 +528,25 @@ int records_par2(p2g_ctx *ctx, const uint16_t *d_consts, const uint32_t *d_exps,
     return P2G_OK;
 }
 
+static int launch_kernel(cudaStream_t stream, const MuladdPlan &p, const uint32_t *planes,
+                         const uint32_t *d_recs, int nin, int nout, int T,
+                         uint8_t *const *d_dst, size_t S, int mode)
+{
+    KernelFn fn = kernel_for(p.warps, p.ereg, p.psplit);
+    size_t smem = smem_bytes(p);
+    P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    long long grid = static_cast<long long>(T) * p.nblk * p.nsplit;
+    if (grid > 0x7fffffffLL) {
+        set_error("muladd grid too large");
+        return P2G_ERANGE;
+    }
+    fn<<<static_cast<unsigned>(grid), p.warps * 32, smem, stream>>>(
+        planes, d_recs, nin, nout, T, p.nblk, p.nsplit, d_dst, S, mode);
+    P2G_CUDA(cudaGetLastError());
+    return P2G_OK;
+}
+
 int muladd_run(p2g_ctx *ctx, const uint8_t *const *d_src, int nin, uint8_t *const *d_dst,
                int nout, size_t S, const uint32_t *d_recs, int mode, const MuladdPlan *plan)
 {
@@ -444,9 +554,9 @@ int muladd_run(p2g_ctx *ctx, const uint8_t *const *d_src, int nin, uint8_t *cons
         return P2G_OK;
     const int T = static_cast<int>((S + kTileBytes - 1) / kTileBytes);
     MuladdPlan p = plan ? *plan : choose_plan(ctx, nin, nout, S);
-    if (p.ereg < 1 || p.ereg > kMaxEreg || p.nblk * kWarps * p.ereg < nout || p.nsplit < 1) {
-        set_error("invalid muladd plan ereg=%d nblk=%d nsplit=%d for %d outputs", p.ereg,
-                  p.nblk, p.nsplit, nout);
+    if (!plan_valid(p, nin, nout, S)) {
+        set_error("invalid muladd plan warps=%d ereg=%d nblk=%d nsplit=%d for %d outputs",
+                  p.warps, p.ereg, p.nblk, p.nsplit, nout);
         return P2G_EINVAL;
     }
     if (nin == 0) {
@@ -473,21 +583,162 @@ int muladd_run(p2g_ctx *ctx, const uint8_t *const *d_src, int nin, uint8_t *cons
         P2G_CUDA(cudaGetLastError());
         ++ctx->launches;
     }
-    KernelFn fn = kernel_for(p.ereg);
-    size_t smem = smem_bytes(p.ereg);
-    P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(smem)));
-    long long grid = static_cast<long long>(T) * p.nblk * p.nsplit;
-    if (grid > 0x7fffffffLL) {
-        set_error("muladd grid too large");
-        return P2G_ERANGE;
-    }
     ctx->mark(2);
-    fn<<<static_cast<unsigned>(grid), kThreads, smem, ctx->stream>>>(
-        planes, d_recs, nin, nout, T, p.nblk, p.nsplit, d_dst, S, mode);
-    P2G_CUDA(cudaGetLastError());
+    P2G_TRY(launch_kernel(ctx->stream, p, planes, d_recs, nin, nout, T, d_dst, S, mode));
     ++ctx->launches;
     ctx->mark(3);
+    return P2G_OK;
+}
+
+// Deterministic pseudo-random bytes for the tuner's synthetic slices.
+__global__ void fill_pattern(uint32_t *p, size_t words, uint32_t seed)
+{
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < words;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        uint32_t x = static_cast<uint32_t>(i) * 0x9E3779B9u ^ seed;
+        x ^= x >> 16;
+        x *= 0x7FEB352Du;
+        x ^= x >> 15;
+        x *= 0x846CA68Bu;
+        x ^= x >> 16;
+        p[i] = x;
+    }
+}
+
+int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdPlan *best,
+                    float *best_ms, int *tried)
+{
+    if (nin <= 0 || nout <= 0 || S == 0 || S % 2) {
+        set_error("p2g_autotune: empty or odd-sized problem");
+        return P2G_EINVAL;
+    }
+    reps = std::max(1, reps);
+    const int T = static_cast<int>((S + kTileBytes - 1) / kTileBytes);
+    const size_t slot = (S + 15) & ~static_cast<size_t>(15);
+    // synthetic sources, outputs, coefficients, records, planes in context scratch
+    P2G_TRY(ctx->in_copy.ensure(slot * nin));
+    P2G_TRY(ctx->out_copy.ensure(slot * nout));
+    P2G_TRY(ctx->coeffs.ensure(static_cast<size_t>(nin) * nout * 2 + 16));
+    P2G_TRY(ctx->recs.ensure(static_cast<size_t>(nin) * nout * 64));
+    P2G_TRY(ctx->planes.ensure(static_cast<size_t>(nin) * T * kTileBytes));
+    fill_pattern<<<1024, 256, 0, ctx->stream>>>(ctx->in_copy.as<uint32_t>(), slot * nin / 4, 1u);
+    fill_pattern<<<256, 256, 0, ctx->stream>>>(ctx->coeffs.as<uint32_t>(),
+                                               static_cast<size_t>(nin) * nout / 2, 7u);
+    P2G_CUDA(cudaGetLastError());
+    std::vector<const uint8_t *> sp(nin);
+    std::vector<uint8_t *> dp(nout);
+    for (int i = 0; i < nin; ++i)
+        sp[i] = ctx->in_copy.as<uint8_t>() + i * slot;
+    for (int o = 0; o < nout; ++o)
+        dp[o] = ctx->out_copy.as<uint8_t>() + o * slot;
+    const size_t ptr_bytes = (static_cast<size_t>(nin) + nout) * sizeof(void *);
+    P2G_TRY(ctx->params.ensure(ptr_bytes));
+    uint8_t *d_ptrs = ctx->params.as<uint8_t>();
+    P2G_CUDA(cudaMemcpyAsync(d_ptrs, sp.data(), nin * sizeof(void *), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    P2G_CUDA(cudaMemcpyAsync(d_ptrs + nin * sizeof(void *), dp.data(), nout * sizeof(void *),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    const uint8_t *const *d_src = reinterpret_cast<const uint8_t *const *>(d_ptrs);
+    uint8_t *const *d_dst = reinterpret_cast<uint8_t *const *>(d_ptrs + nin * sizeof(void *));
+    P2G_TRY(records_from_matrix(ctx, ctx->coeffs.as<uint16_t>(), nin, nout, ctx->recs.as<uint32_t>()));
+    size_t groups = static_cast<size_t>(nin) * T * 32;
+    slices_to_planes<<<static_cast<unsigned>((groups + 255) / 256), 256, 0, ctx->stream>>>(
+        d_src, nin, T, S, ctx->planes.as<uint32_t>());
+    P2G_CUDA(cudaGetLastError());
+
+    // candidates: each compiled (warps, ereg) shape at the fewest output blocks
+    // it allows and the next two, times input splits that keep the grid
+    // within a few waves
+    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    std::vector<MuladdPlan> cands;
+    for (const Variant &v0 : kVariants) {
+        // one pass per (warps, psplit) family: its largest compiled ereg
+        // sets the fewest output blocks; then the next two block counts, each
+        // with the smallest compiled ereg that covers nout
+        bool first = true;
+        int emax = 0;
+        for (const Variant &v : kVariants) {
+            if (v.warps == v0.warps && v.psplit == v0.psplit) {
+                emax = std::max(emax, v.ereg);
+                if (&v < &v0)
+                    first = false;
+            }
+        }
+        if (!first)
+            continue;
+        const int G = v0.warps / v0.psplit;
+        const int nmin = (nout + G * emax - 1) / (G * emax);
+        for (int nblk = nmin; nblk <= nmin + 2; ++nblk) {
+            const int need = (nout + G * nblk - 1) / (G * nblk);
+            int ereg = 0;
+            for (const Variant &v : kVariants)
+                if (v.warps == v0.warps && v.psplit == v0.psplit && v.ereg >= need &&
+                    (ereg == 0 || v.ereg < ereg))
+                    ereg = v.ereg;
+            if (ereg == 0)
+                continue;
+            MuladdPlan p;
+            p.warps = v0.warps;
+            p.psplit = v0.psplit;
+            p.ereg = ereg;
+            p.nblk = nblk;
+            for (int ns : {1, 2, 3, 4, 6, 8}) {
+                p.nsplit = ns;
+                const long long ctas = static_cast<long long>(T) * nblk * ns;
+                if (ns > 1 && (nin / ns < 8 || ctas > 8LL * sms))
+                    continue;
+                if (!plan_valid(p, nin, nout, S))
+                    continue;
+                bool dup = false;
+                for (const MuladdPlan &q : cands)
+                    dup = dup || (q.warps == p.warps && q.ereg == p.ereg && q.nblk == p.nblk &&
+                                  q.nsplit == p.nsplit && q.psplit == p.psplit);
+                if (!dup)
+                    cands.push_back(p);
+            }
+        }
+    }
+    cudaEvent_t e0, e1;
+    P2G_CUDA(cudaEventCreate(&e0));
+    P2G_CUDA(cudaEventCreate(&e1));
+    float best_t = 1e30f;
+    MuladdPlan best_p = choose_plan(nullptr, nin, nout, S);
+    int rc = P2G_OK;
+    for (const MuladdPlan &p : cands) {
+        // warm-up launch, then the best of `reps` timed launches
+        rc = launch_kernel(ctx->stream, p, ctx->planes.as<uint32_t>(), ctx->recs.as<uint32_t>(),
+                           nin, nout, T, d_dst, S, 1);
+        if (rc != P2G_OK)
+            break;
+        float t = 1e30f;
+        for (int r = 0; r < reps && rc == P2G_OK; ++r) {
+            cudaEventRecord(e0, ctx->stream);
+            rc = launch_kernel(ctx->stream, p, ctx->planes.as<uint32_t>(),
+                               ctx->recs.as<uint32_t>(), nin, nout, T, d_dst, S, 1);
+            cudaEventRecord(e1, ctx->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                set_error("p2g_autotune: %s", cudaGetErrorString(cudaGetLastError()));
+                rc = P2G_ECUDA;
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t = std::min(t, ms);
+        }
+        if (rc != P2G_OK)
+            break;
+        if (t < best_t) {
+            best_t = t;
+            best_p = p;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    P2G_TRY(rc);
+    ctx->plans[plan_key(nin, nout, S)] = best_p;
+    *best = best_p;
+    *best_ms = best_t;
+    *tried = static_cast<int>(cands.size());
     return P2G_OK;
 }
 
@@ -529,12 +780,12 @@ int muladd_run_fixed(cudaStream_t stream, int sm_count, const uint8_t *const *d_
     slices_to_planes<<<static_cast<unsigned>((groups + 255) / 256), 256, 0, stream>>>(
         d_src, nin, T, S, d_planes);
     P2G_CUDA(cudaGetLastError());
-    KernelFn fn = kernel_for(p.ereg);
-    size_t smem = smem_bytes(p.ereg);
+    KernelFn fn = kernel_for(p.warps, p.ereg, p.psplit);
+    size_t smem = smem_bytes(p);
     P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
     long long grid = static_cast<long long>(T) * p.nblk * p.nsplit;
-    fn<<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(
+    fn<<<static_cast<unsigned>(grid), p.warps * 32, smem, stream>>>(
         d_planes, d_recs, nin, nout, T, p.nblk, p.nsplit, d_dst, S, 0);
     P2G_CUDA(cudaGetLastError());
     return P2G_OK;

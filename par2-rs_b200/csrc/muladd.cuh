@@ -4,15 +4,18 @@
 
 namespace p2g {
 
-// How one muladd problem is cut into CTAs (chosen by choose_plan or by the
-// autotuner): outputs per warp, output blocks, input splits.
-struct MuladdPlan {
-    int ereg = 1;    // outputs per warp (accumulators: 16 registers each)
-    int nblk = 1;    // output blocks of 8*ereg outputs
-    int nsplit = 1;  // input ranges reduced with atomic XOR
-};
-
+// The plan for a problem: the context's tuned plan for this shape if there
+// is one, else a heuristic (8 warps, as many outputs per warp as fit).
 MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t slice_bytes);
+bool plan_valid(const MuladdPlan &p, int nin, int nout, size_t slice_bytes);
+// The compiled (warps, outputs per group, warps per group) shapes; returns
+// their number.
+int muladd_variants(int *warps, int *eregs, int *psplits, int cap);
+
+// Times every candidate plan for (nin, nout, S) on synthetic data in the
+// context's scratch, caches the fastest in ctx->plans and returns it.
+int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdPlan *best,
+                    float *best_ms, int *tried);
 
 // Coefficient records [nin][nout][16 words] from a row-major matrix
 // coeff[nout][nin] (coefficients[dst][src] of galois/region/mod.rs:78-82).

@@ -42,6 +42,8 @@ SIGNATURES = [
     ("p2g_set_stream", _I, [_P, _P]),
     ("p2g_set_timing", _I, [_P, _I]),
     ("p2g_last_timing", _I, [_P, _P]),
+    ("p2g_autotune", _I, [_P, _S, _S, _S, _I, _P]),
+    ("p2g_set_plan", _I, [_P, _S, _S, _S, _P]),
     ("p2g_strategy_info", _I, [_P, _P, _P]),
     ("p2g_mul_slice", _I, [_P, _U16, _P, _S, _U32]),
     ("p2g_muladd", _I, [_P, _P, _P, _S, _U16, _U32]),
@@ -63,6 +65,16 @@ class Timing(ctypes.Structure):
     _fields_ = [("ms_records", ctypes.c_float), ("ms_planes", ctypes.c_float),
                 ("ms_kernel", ctypes.c_float), ("ms_total", ctypes.c_float),
                 ("launches", ctypes.c_int)]
+
+
+class Plan(ctypes.Structure):
+    """p2g_plan: tile shape of the multiply-accumulate kernel."""
+    _fields_ = [("warps", ctypes.c_int), ("outputs_per_group", ctypes.c_int),
+                ("warps_per_group", ctypes.c_int), ("output_blocks", ctypes.c_int),
+                ("input_splits", ctypes.c_int), ("ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class Par2GpuError(RuntimeError):
@@ -176,6 +188,18 @@ class Context:
         t = Timing()
         check(lib().p2g_last_timing(self.h, ctypes.byref(t)))
         return t
+
+    def autotune(self, nin, nout, slice_bytes, reps=2):
+        """Time the kernel's tile shapes for this problem shape and keep the
+        fastest as this context's plan for it; returns the Plan."""
+        p = Plan()
+        check(lib().p2g_autotune(self.h, nin, nout, slice_bytes, reps, ctypes.byref(p)))
+        return p
+
+    def set_plan(self, nin, nout, slice_bytes, warps, outputs_per_group, output_blocks,
+                 input_splits=1, warps_per_group=1):
+        p = Plan(warps, outputs_per_group, warps_per_group, output_blocks, input_splits, 0.0)
+        check(lib().p2g_set_plan(self.h, nin, nout, slice_bytes, ctypes.byref(p)))
 
     # --- GaloisSimdStrategy mirror (galois/simd/mod.rs:36-58) -------------
     def mul_slice(self, scalar, data, device=False):

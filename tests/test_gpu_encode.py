@@ -129,3 +129,45 @@ def test_bad_arguments_report_errors(ctx):
         ctx.encode([src[0], src[1]], 7, [0], [np.zeros(7, np.uint8)])
     assert ei.value.code == par2gpu.EINVAL
     assert "even" in par2gpu.last_error()
+
+
+VARIANTS = [(8, e, 1) for e in range(1, 14)] + [(12, e, 1) for e in (4, 6, 7, 8)] + \
+    [(16, e, 1) for e in (2, 3, 4, 5)] + [(16, e, 2) for e in (8, 10, 12, 13)]
+
+
+def test_every_tile_shape_matches_oracle(ctx):
+    """Each compiled (warps, outputs per warp) shape, with and without input
+    splits, gives the oracle's recovery slices."""
+    rng = np.random.default_rng(31)
+    k, S, r = 40, 2048 * 5 + 64, 50
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(r, dtype=np.uint32)
+    want = oracle.encode(src, exps)
+    for W, E, P in VARIANTS:
+        G = W // P
+        nblk = -(-r // (G * E))
+        if (nblk - 1) * G * E >= r:
+            continue
+        for ns in (1, 3):
+            ctx.set_plan(k, r, S, W, E, nblk, ns, P)
+            got = ctx.encode_array(src, exps)
+            assert np.array_equal(got, want), (W, E, P, nblk, ns)
+
+
+def test_autotune_picks_a_correct_plan(ctx):
+    rng = np.random.default_rng(32)
+    k, S, r = 300, 16384, 37
+    plan = ctx.autotune(k, r, S)
+    assert plan.warps in (8, 12, 16) and plan.ms > 0
+    assert plan.output_blocks * plan.warps // plan.warps_per_group * plan.outputs_per_group >= r
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(r, dtype=np.uint32)
+    assert np.array_equal(ctx.encode_array(src, exps), oracle.encode(src, exps))
+
+
+def test_set_plan_rejects_uncompiled_shapes(ctx):
+    import par2gpu
+
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        ctx.set_plan(10, 20, 4096, 16, 9, 1, 1)
+    assert ei.value.code == par2gpu.EINVAL
