@@ -4,6 +4,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
@@ -286,9 +287,16 @@ int p2g_create(int device, p2g_ctx **out)
             break;
         }
         ctx->stream = ctx->own_stream;
+        if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            set_error("cudaStreamCreate failed");
+            rc = P2G_ECUDA;
+            break;
+        }
         bool ev_ok = true;
         for (cudaEvent_t &e : ctx->ev)
             ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
+        for (cudaEvent_t &e : ctx->pipe_ev)
+            ev_ok = ev_ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
         if (!ev_ok) {
             set_error("cudaEventCreate failed");
             rc = P2G_ECUDA;
@@ -352,6 +360,13 @@ int p2g_destroy(p2g_ctx *ctx)
     for (cudaEvent_t e : ctx->ev)
         if (e)
             cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->pipe_ev)
+        if (e)
+            cudaEventDestroy(e);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
     if (ctx->own_stream)
         cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -479,9 +494,12 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     P2G_CUDA(cudaSetDevice(ctx->device));
     begin(ctx);
     const bool dev = flags & P2G_DEVICE_PTRS;
+    // Host sources are copied in groups on the copy stream while the kernel
+    // accumulates the groups already on the device (XOR into the outputs).
+    const int groups = (!dev && k >= 128) ? static_cast<int>(std::min<size_t>(p2g_ctx::kPipe, k / 64)) : 1;
     std::vector<uint8_t *> s, d;
     bool s_staged = false, d_staged = false;
-    P2G_TRY(stage(ctx, ctx->in_copy, src, k, slice_bytes, dev, true, s, s_staged));
+    P2G_TRY(stage(ctx, ctx->in_copy, src, k, slice_bytes, dev, groups == 1, s, s_staged));
     P2G_TRY(stage(ctx, ctx->out_copy, out, r, slice_bytes, dev, false, d, d_staged));
     ParamLayout L(k, r, k * 2, r * 4);
     P2G_TRY(ctx->hparams.ensure(L.total));
@@ -497,9 +515,28 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     P2G_TRY(records_par2(ctx, reinterpret_cast<const uint16_t *>(dp + L.a_off),
                          reinterpret_cast<const uint32_t *>(dp + L.b_off), static_cast<int>(k),
                          static_cast<int>(r), ctx->recs.as<uint32_t>()));
-    P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.src_off),
-                       static_cast<int>(k), reinterpret_cast<uint8_t *const *>(dp + L.dst_off),
-                       static_cast<int>(r), slice_bytes, ctx->recs.as<uint32_t>(), 0));
+    const uint8_t *const *d_src = reinterpret_cast<const uint8_t *const *>(dp + L.src_off);
+    uint8_t *const *d_dst = reinterpret_cast<uint8_t *const *>(dp + L.dst_off);
+    if (groups == 1) {
+        P2G_TRY(muladd_run(ctx, d_src, static_cast<int>(k), d_dst, static_cast<int>(r),
+                           slice_bytes, ctx->recs.as<uint32_t>(), 0));
+    } else {
+        // the copy stream starts after everything already queued on the
+        // compute stream (earlier users of the staging buffers)
+        P2G_CUDA(cudaEventRecord(ctx->pipe_ev[0], ctx->stream));
+        P2G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ev[0], 0));
+        for (int g = 0; g < groups; ++g) {
+            const size_t i0 = k * g / groups, i1 = k * (g + 1) / groups;
+            for (size_t i = i0; i < i1; ++i)
+                P2G_CUDA(cudaMemcpyAsync(s[i], src[i], slice_bytes, cudaMemcpyHostToDevice,
+                                         ctx->copy_stream));
+            P2G_CUDA(cudaEventRecord(ctx->pipe_ev[g], ctx->copy_stream));
+            P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
+            P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
+                               static_cast<int>(r), slice_bytes,
+                               ctx->recs.as<uint32_t>() + i0 * r * 16, g == 0 ? 0 : 1));
+        }
+    }
     if (d_staged)
         P2G_TRY(unstage(ctx, out, d, r, slice_bytes, dev));
     return finish(ctx);

@@ -436,7 +436,7 @@ static const Variant kVariants[] = {
     P2G_V(8, 6, 1),   P2G_V(8, 7, 1),   P2G_V(8, 8, 1),   P2G_V(8, 9, 1),   P2G_V(8, 10, 1),
     P2G_V(8, 11, 1),  P2G_V(8, 12, 1),  P2G_V(8, 13, 1),  P2G_V(12, 4, 1),  P2G_V(12, 6, 1),
     P2G_V(12, 7, 1),  P2G_V(12, 8, 1),  P2G_V(16, 2, 1),  P2G_V(16, 3, 1),  P2G_V(16, 4, 1),
-    P2G_V(16, 5, 1),  P2G_V(16, 8, 2),  P2G_V(16, 10, 2), P2G_V(16, 12, 2), P2G_V(16, 13, 2),
+    P2G_V(16, 5, 1),  P2G_V(16, 8, 2),  P2G_V(16, 10, 2), P2G_V(16, 12, 2),
 };
 #undef P2G_V
 
