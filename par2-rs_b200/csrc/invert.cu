@@ -16,7 +16,12 @@
 // the pivot's inverse) and gj_eliminate (one CTA per row: row ^= f * pivot
 // row).  A status word turns the remaining steps into no-ops once a column has
 // no pivot.
+#include <algorithm>
+#include <vector>
+
+#include "bitslice.cuh"
 #include "invert.cuh"
+#include "muladd.cuh"
 
 namespace p2g {
 
@@ -64,95 +69,385 @@ __global__ void gj_build_from(uint16_t *__restrict__ M, int m, int W, const uint
             col < m ? A[static_cast<size_t>(row) * m + col] : static_cast<uint16_t>(col - m == row);
 }
 
-__global__ void gj_pivot(uint16_t *__restrict__ M, int m, int W, int k,
-                         const uint16_t *__restrict__ glog, const uint16_t *__restrict__ gexp,
-                         int *__restrict__ status, uint16_t *__restrict__ pivots)
+// a * b without tables: carry-less shift-and-add with reduction by
+// x^16 + x^12 + x^3 + x + 1 at every step (no memory latency on the
+// sequential paths of the pivot search).
+__device__ __forceinline__ uint32_t gmul_alu(uint32_t a, uint32_t b)
 {
-    __shared__ int found;
-    if (*status != 0)
-        return;
-    uint16_t *rowk = M + static_cast<size_t>(k) * W;
-    if (threadIdx.x == 0)
-        found = rowk[k] != 0 ? k : m;
-    __syncthreads();
-    if (found == m) {
-        // first row below k with a non-zero entry in column k (par2_rs.rs:361-370)
-        for (int r = k + 1 + threadIdx.x; r < m; r += blockDim.x)
-            if (M[static_cast<size_t>(r) * W + k] != 0)
-                atomicMin(&found, r);
-        __syncthreads();
-        if (found == m) {
-            if (threadIdx.x == 0)
-                *status = 1;  // singular
-            return;
-        }
-        uint16_t *rowr = M + static_cast<size_t>(found) * W;
-        for (int j = threadIdx.x; j < 2 * m; j += blockDim.x) {
-            uint16_t t = rowk[j];
-            rowk[j] = rowr[j];
-            rowr[j] = t;
-        }
-        __syncthreads();
+    uint32_t r = 0;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        r ^= a & (0u - ((b >> i) & 1u));
+        a = (a << 1) ^ ((a & 0x8000u) ? 0x1100Bu : 0u);
     }
-    const uint32_t p = rowk[k];
-    __syncthreads();
-    if (threadIdx.x == 0)
-        pivots[k] = static_cast<uint16_t>(p);
+    return r & 0xFFFFu;
+}
+
+__device__ __forceinline__ uint32_t ginv(uint32_t p, const uint16_t *__restrict__ glog,
+                                         const uint16_t *__restrict__ gexp)
+{
     // p^-1 = 2^(65535 - log p)
     const uint32_t lp = glog[p];
-    const uint32_t pinv = gexp[lp == 0 ? 0 : 65535u - lp];
-    for (int j = k + threadIdx.x; j < 2 * m; j += blockDim.x)
-        rowk[j] = static_cast<uint16_t>(gmul(rowk[j], pinv, glog, gexp));
+    return gexp[lp == 0 ? 0 : 65535u - lp];
 }
 
-__global__ void gj_eliminate(uint16_t *__restrict__ M, int m, int W, int k,
-                             const uint16_t *__restrict__ glog, const uint16_t *__restrict__ gexp,
-                             const int *__restrict__ status)
+constexpr int kSmallM = 96;   // matrices up to this size: one CTA, all in shared memory
+constexpr int kPanel = 64;    // panel width of the blocked elimination
+constexpr int kGjThreads = 256;
+
+// Gauss-Jordan on [A | I] (n x 2n, row stride ld) in shared memory by one
+// CTA, with the reference's pivot rule: rows are swapped only when the
+// diagonal entry is zero (first non-zero row below).  Returns false (for every
+// thread) when A is singular.
+__device__ bool cta_gauss_jordan(uint16_t *S, int n, int ld, uint32_t *fcol,
+                                 const uint16_t *__restrict__ glog,
+                                 const uint16_t *__restrict__ gexp)
 {
-    const int r = blockIdx.x;
-    if (*status != 0 || r == k)
-        return;
-    __shared__ uint32_t f;
-    uint16_t *row = M + static_cast<size_t>(r) * W;
-    const uint16_t *rowk = M + static_cast<size_t>(k) * W;
-    if (threadIdx.x == 0)
-        f = row[k];
+    __shared__ int piv;
+    const int tid = threadIdx.x, nt = blockDim.x, w2 = 2 * n;
+    for (int k = 0; k < n; ++k) {
+        if (tid == 0)
+            piv = n;
+        __syncthreads();
+        // first row r >= k with a non-zero entry in column k
+        for (int r0 = k; r0 < n; r0 += nt) {
+            const int r = r0 + tid;
+            const bool nz = r < n && S[r * ld + k] != 0;
+            const unsigned ball = __ballot_sync(0xffffffffu, nz);
+            if (ball && (tid & 31) == 0)
+                atomicMin(&piv, r0 + (tid & ~31) + __ffs(ball) - 1);
+            __syncthreads();
+            if (piv < n)
+                break;
+        }
+        if (tid == 0 && piv == n)
+            piv = -1;
+        __syncthreads();
+        const int p = piv;
+        if (p < 0)
+            return false;
+        if (p != k) {
+            for (int j = tid; j < w2; j += nt) {
+                uint16_t t = S[k * ld + j];
+                S[k * ld + j] = S[p * ld + j];
+                S[p * ld + j] = t;
+            }
+            __syncthreads();
+        }
+        const uint32_t pinv = ginv(S[k * ld + k], glog, gexp);
+        __syncthreads();
+        for (int j = tid; j < w2; j += nt)
+            S[k * ld + j] = static_cast<uint16_t>(gmul_alu(S[k * ld + j], pinv));
+        __syncthreads();
+        for (int r = tid; r < n; r += nt)
+            fcol[r] = r == k ? 0u : S[r * ld + k];
+        __syncthreads();
+        for (int idx = tid; idx < n * w2; idx += nt) {
+            const int r = idx / w2, j = idx - r * w2;
+            const uint32_t f = fcol[r];
+            if (f)
+                S[r * ld + j] ^= static_cast<uint16_t>(gmul_alu(f, S[k * ld + j]));
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+// Whole inversion of a small matrix (m <= kSmallM) by one CTA.
+__global__ void __launch_bounds__(kGjThreads)
+    gj_small(const uint16_t *__restrict__ M, int m, int W, uint16_t *__restrict__ inv,
+             int *__restrict__ status, const uint16_t *__restrict__ glog,
+             const uint16_t *__restrict__ gexp)
+{
+    extern __shared__ uint16_t S[];  // m x 2m
+    __shared__ uint32_t fcol[kSmallM];
+    for (int idx = threadIdx.x; idx < m * 2 * m; idx += blockDim.x) {
+        const int r = idx / (2 * m), j = idx - r * 2 * m;
+        S[idx] = M[static_cast<size_t>(r) * W + j];
+    }
     __syncthreads();
-    const uint32_t fr = f;
-    if (fr == 0)
+    if (!cta_gauss_jordan(S, m, 2 * m, fcol, glog, gexp)) {
+        if (threadIdx.x == 0)
+            *status = 1;
         return;
-    const uint32_t lf = glog[fr];
-    for (int j = k + threadIdx.x; j < 2 * m; j += blockDim.x) {
-        uint32_t x = rowk[j];
-        if (x) {
-            uint32_t l = glog[x] + lf;
-            if (l >= 65535u)
-                l -= 65535u;
-            row[j] ^= gexp[l];
+    }
+    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+        const int r = idx / m, j = idx - r * m;
+        inv[idx] = S[r * 2 * m + m + j];
+    }
+}
+
+// Scratch of the blocked elimination (device).
+struct PanelBufs {
+    uint16_t *akk_inv;  // kPanel x kPanel inverse of the pivot block
+    int *used;          // m: row already a pivot row
+    int *kall;          // m: pivot row of each column
+    int *orow;          // m: the rows that are not this panel's pivots
+    const uint8_t **kptr;  // kPanel row pointers of the pivot rows
+    uint8_t **optr;        // m row pointers of the other rows
+};
+
+// One panel [c0, c0+b) of the blocked Gauss-Jordan, by one CTA: choose b
+// pivot rows among the rows not yet used (incremental row reduction,
+// smallest row index first), invert their b x b block A_KK, and list
+// the pivot rows (K) and the other rows (O) for the two multiply-accumulate
+// passes that follow:  X = A_KK^-1 M[K,:];  M[O,:] ^= M[O, panel] X;  M[K,:] = X.
+// On a singular matrix (or after an earlier failure) it sets *status and
+// still writes valid row lists so the passes stay in bounds.
+__global__ void __launch_bounds__(kGjThreads)
+    gj_panel(uint16_t *__restrict__ M, int m, int W, int c0, int b, PanelBufs pb,
+             int *__restrict__ status, const uint16_t *__restrict__ glog,
+             const uint16_t *__restrict__ gexp)
+{
+    __shared__ uint16_t S[kPanel * 2 * kPanel];
+    __shared__ uint32_t fcol[kPanel];
+    __shared__ int ksel[kPanel];
+    __shared__ int failed;
+    __shared__ int scan[kGjThreads];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0)
+        failed = *status != 0;
+    __syncthreads();
+    if (!failed) {
+        // Incremental row reduction: candidate rows (unused, ascending) are
+        // reduced against the pivot rows found so far (kept in reduced echelon
+        // form, pivot entries 1); a candidate with a non-zero remainder
+        // becomes the pivot of its first non-zero column.  Stops after b
+        // pivots, so only about b rows are touched per panel.
+        uint16_t *piv_rows = S;           // b x kPanel (reuses the A_KK buffer)
+        __shared__ uint16_t vec[kPanel];
+        __shared__ uint16_t coef[kPanel];                // f_q or g_q of the current step
+        __shared__ uint16_t part[kGjThreads / kPanel][kPanel];
+        __shared__ int piv_col[kPanel];
+        __shared__ int nk, cand, lead;
+        // used[] as a bitmap (m <= 65535 rows)
+        __shared__ uint32_t used_bits[65536 / 32];
+        const int nwords = (m + 31) / 32;
+        for (int w = tid; w < nwords; w += nt) {
+            uint32_t bits = 0;
+            for (int i = 0; i < 32 && w * 32 + i < m; ++i)
+                bits |= pb.used[w * 32 + i] ? (1u << i) : 0u;
+            used_bits[w] = bits;
+        }
+        constexpr int QG = kGjThreads / kPanel;          // pivot groups summed in parallel
+        const int col = tid % kPanel, qg = tid / kPanel;
+        if (tid == 0) {
+            nk = 0;
+            cand = -1;
+        }
+        __syncthreads();
+        while (true) {
+            if (tid == 0) {
+                // next row after cand whose used bit is clear
+                int r = cand + 1, found = m;
+                for (int w = r >> 5; w < nwords; ++w) {
+                    uint32_t free_bits = ~used_bits[w];
+                    if (w == (r >> 5))
+                        free_bits &= ~0u << (r & 31);
+                    if (free_bits) {
+                        found = min(m, w * 32 + __ffs(free_bits) - 1);
+                        break;
+                    }
+                }
+                cand = found;
+            }
+            __syncthreads();
+            const int r = cand;
+            if (r >= m || nk >= b)
+                break;
+            const int n0 = nk;
+            if (tid < b)
+                vec[tid] = M[static_cast<size_t>(r) * W + c0 + tid];
+            __syncthreads();
+            // The pivot rows are reduced (zero in every other pivot column), so
+            // the coefficients of all reductions are the candidate's own
+            // entries in the pivot columns: one dot product, no chain.
+            if (tid < n0)
+                coef[tid] = vec[piv_col[tid]];
+            __syncthreads();
+            {
+                uint32_t acc = 0;
+                if (col < b)
+                    for (int q = qg; q < n0; q += QG)
+                        acc ^= gmul_alu(coef[q], piv_rows[q * kPanel + col]);
+                part[qg][col] = static_cast<uint16_t>(acc);
+            }
+            __syncthreads();
+            if (tid < b) {
+                uint32_t x = vec[tid];
+#pragma unroll
+                for (int g2 = 0; g2 < QG; ++g2)
+                    x ^= part[g2][tid];
+                vec[tid] = static_cast<uint16_t>(x);
+            }
+            __syncthreads();
+            if (tid < 64) {
+                const unsigned ball = __ballot_sync(0xffffffffu, tid < b && vec[tid] != 0);
+                if ((tid & 31) == 0)
+                    part[0][tid >> 5] = static_cast<uint16_t>(ball ? (tid + __ffs(ball) - 1) : 0xFFFF);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                const int a0 = part[0][0], a1 = part[0][1];
+                lead = a0 != 0xFFFF ? a0 : (a1 != 0xFFFF ? a1 : b);
+            }
+            __syncthreads();
+            const int j = lead;
+            if (j < b) {
+                const uint32_t inv = ginv(vec[j], glog, gexp);
+                if (tid < n0)
+                    coef[tid] = piv_rows[tid * kPanel + j];
+                __syncthreads();
+                if (tid < b)
+                    vec[tid] = static_cast<uint16_t>(gmul_alu(vec[tid], inv));
+                __syncthreads();
+                // keep the earlier pivot rows reduced in the new pivot column
+                for (int idx = tid; idx < n0 * kPanel; idx += nt) {
+                    const int q = idx / kPanel, c = idx - q * kPanel;
+                    if (c < b && coef[q])
+                        piv_rows[q * kPanel + c] ^= static_cast<uint16_t>(gmul_alu(coef[q], vec[c]));
+                }
+                if (tid < b)
+                    piv_rows[n0 * kPanel + tid] = vec[tid];
+                if (tid == 0) {
+                    piv_col[n0] = j;
+                    ksel[n0] = r;
+                    pb.used[r] = 1;
+                    used_bits[r >> 5] |= 1u << (r & 31);
+                    nk = n0 + 1;
+                }
+            }
+            __syncthreads();
+        }
+        if (nk < b) {
+            if (tid == 0)
+                failed = 1;
+            __syncthreads();
+        }
+    }
+    if (failed) {
+        // valid but meaningless row lists
+        for (int j = tid; j < b; j += nt)
+            ksel[j] = j;
+        if (tid == 0)
+            *status = 1;
+        __syncthreads();
+    } else {
+        // A_KK^-1 from the current values of the pivot rows' panel columns
+        for (int idx = tid; idx < b * 2 * b; idx += nt) {
+            const int r = idx / (2 * b), j = idx - r * 2 * b;
+            S[r * 2 * kPanel + j] =
+                j < b ? M[static_cast<size_t>(ksel[r]) * W + c0 + j]
+                      : static_cast<uint16_t>(j - b == r);
+        }
+        __syncthreads();
+        if (!cta_gauss_jordan(S, b, 2 * kPanel, fcol, glog, gexp)) {
+            // cannot happen when every column found a pivot; guarded anyway
+            if (tid == 0)
+                *status = 1;
+        }
+        for (int idx = tid; idx < b * b; idx += nt) {
+            const int r = idx / b, j = idx - r * b;
+            pb.akk_inv[idx] = S[r * 2 * kPanel + b + j];
+        }
+    }
+    for (int j = tid; j < b; j += nt) {
+        pb.kptr[j] = reinterpret_cast<const uint8_t *>(M + static_cast<size_t>(ksel[j]) * W);
+        pb.kall[c0 + j] = ksel[j];
+    }
+    // O = rows not in K, ascending: block-wide exclusive scan of the flags
+    const int per = (m + nt - 1) / nt, r0 = tid * per, r1 = min(m, r0 + per);
+    auto in_k = [&](int r) {
+        for (int j = 0; j < b; ++j)
+            if (ksel[j] == r)
+                return true;
+        return false;
+    };
+    int cnt = 0;
+    for (int r = r0; r < r1; ++r)
+        cnt += !in_k(r);
+    scan[tid] = cnt;
+    __syncthreads();
+    if (tid == 0) {
+        int acc = 0;
+        for (int t = 0; t < nt; ++t) {
+            int c = scan[t];
+            scan[t] = acc;
+            acc += c;
+        }
+    }
+    __syncthreads();
+    int o = scan[tid];
+    for (int r = r0; r < r1; ++r) {
+        if (!in_k(r)) {
+            pb.orow[o] = r;
+            pb.optr[o] = reinterpret_cast<uint8_t *>(M + static_cast<size_t>(r) * W);
+            ++o;
         }
     }
 }
 
-// Copies the right half of [I | A^-1] into a dense m x m matrix.
-__global__ void gj_extract(const uint16_t *__restrict__ M, int m, int W, uint16_t *__restrict__ inv)
+// Records for the row update: coefficient (i, o) = M[orow[o]][c0 + i].
+__global__ void gj_records_rows(const uint16_t *__restrict__ M, int W, const int *__restrict__ orow,
+                                int c0, int nin, int nout, uint32_t *__restrict__ recs)
 {
-    int row = blockIdx.y;
-    for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < m; col += gridDim.x * blockDim.x)
-        inv[static_cast<size_t>(row) * m + col] = M[static_cast<size_t>(row) * W + m + col];
+    size_t gid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gid >= static_cast<size_t>(nin) * nout)
+        return;
+    const int o = static_cast<int>(gid % nout), i = static_cast<int>(gid / nout);
+    uint32_t w[16];
+    make_record(M[static_cast<size_t>(orow[o]) * W + c0 + i], w);
+    uint4 *R = reinterpret_cast<uint4 *>(recs + gid * 16);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        R[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
 }
+
+// M[K_j, :] = X_j
+__global__ void gj_copy_rows(const uint8_t *const *__restrict__ xptr,
+                             const uint8_t *const *__restrict__ kptr, int b, size_t bytes)
+{
+    const int j = blockIdx.y;
+    if (j >= b)
+        return;
+    const uint4 *x = reinterpret_cast<const uint4 *>(xptr[j]);
+    uint4 *k = reinterpret_cast<uint4 *>(const_cast<uint8_t *>(kptr[j]));
+    for (size_t q = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < bytes / 16;
+         q += static_cast<size_t>(gridDim.x) * blockDim.x)
+        k[q] = x[q];
+}
+
+// inv[c][:] = right half of row kall[c]
+__global__ void gj_extract_perm(const uint16_t *__restrict__ M, int m, int W,
+                                const int *__restrict__ kall, uint16_t *__restrict__ inv)
+{
+    const int c = blockIdx.y;
+    const uint16_t *row = M + static_cast<size_t>(kall[c]) * W + m;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x)
+        inv[static_cast<size_t>(c) * m + j] = row[j];
+}
+
+static size_t al256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
 
 int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uint32_t *d_exps,
               const uint16_t *d_A, uint16_t *d_inv)
 {
     if (m <= 0)
         return P2G_OK;
-    const int W = (2 * m + 7) & ~7;
-    P2G_TRY(w.M.ensure(static_cast<size_t>(m) * W * 2));
-    P2G_TRY(w.status.ensure(sizeof(int) + static_cast<size_t>(m) * 2 + 16));
+    const int W = (2 * m + 7) & ~7;  // row stride in u16: rows are 16-byte aligned
+    const size_t row_bytes = static_cast<size_t>(W) * 2;
+    P2G_TRY(w.M.ensure(static_cast<size_t>(m) * row_bytes));
+    // aux layout: status | used | kall | orow | kptr | optr | xptr | akk_inv | X
+    const size_t o_used = 256, o_kall = o_used + al256(m * 4), o_orow = o_kall + al256(m * 4),
+                 o_kptr = o_orow + al256(m * 4), o_optr = o_kptr + al256(kPanel * 8),
+                 o_xptr = o_optr + al256(static_cast<size_t>(m) * 8),
+                 o_akk = o_xptr + al256(kPanel * 8),
+                 o_X = o_akk + al256(kPanel * kPanel * 2), total = o_X + kPanel * row_bytes;
+    P2G_TRY(w.status.ensure(total));
+    uint8_t *aux = w.status.as<uint8_t>();
     uint16_t *M = w.M.as<uint16_t>();
-    int *status = w.status.as<int>();
-    uint16_t *pivots = reinterpret_cast<uint16_t *>(w.status.as<uint8_t>() + 16);
-    P2G_CUDA(cudaMemsetAsync(status, 0, sizeof(int), ctx->stream));
+    int *status = reinterpret_cast<int *>(aux);
+    P2G_CUDA(cudaMemsetAsync(aux, 0, o_kall, ctx->stream));  // status + used
     dim3 g(static_cast<unsigned>((2 * m + 255) / 256 < 64 ? (2 * m + 255) / 256 : 64),
            static_cast<unsigned>(m));
     if (d_A)
@@ -161,13 +456,59 @@ int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uin
         gj_build_par2<<<g, 256, 0, ctx->stream>>>(M, m, W, d_cmiss, d_exps, ctx->d_log, ctx->d_exp);
     P2G_CUDA(cudaGetLastError());
     ++ctx->launches;
-    for (int k = 0; k < m; ++k) {
-        gj_pivot<<<1, 256, 0, ctx->stream>>>(M, m, W, k, ctx->d_log, ctx->d_exp, status, pivots);
-        gj_eliminate<<<m, 128, 0, ctx->stream>>>(M, m, W, k, ctx->d_log, ctx->d_exp, status);
-        ctx->launches += 2;
+    if (m <= kSmallM) {
+        const size_t smem = static_cast<size_t>(m) * 2 * m * 2;
+        gj_small<<<1, kGjThreads, smem, ctx->stream>>>(M, m, W, d_inv, status, ctx->d_log,
+                                                      ctx->d_exp);
+        P2G_CUDA(cudaGetLastError());
+        ++ctx->launches;
+        return P2G_OK;
     }
-    P2G_CUDA(cudaGetLastError());
-    gj_extract<<<g, 256, 0, ctx->stream>>>(M, m, W, d_inv);
+    PanelBufs pb;
+    pb.used = reinterpret_cast<int *>(aux + o_used);
+    pb.kall = reinterpret_cast<int *>(aux + o_kall);
+    pb.orow = reinterpret_cast<int *>(aux + o_orow);
+    pb.kptr = reinterpret_cast<const uint8_t **>(aux + o_kptr);
+    pb.optr = reinterpret_cast<uint8_t **>(aux + o_optr);
+    uint8_t **xptr = reinterpret_cast<uint8_t **>(aux + o_xptr);
+    pb.akk_inv = reinterpret_cast<uint16_t *>(aux + o_akk);
+    uint8_t *X = aux + o_X;
+    {
+        std::vector<uint8_t *> xp(kPanel);
+        for (int j = 0; j < kPanel; ++j)
+            xp[j] = X + j * row_bytes;
+        P2G_CUDA(cudaMemcpyAsync(xptr, xp.data(), kPanel * sizeof(void *), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        // pageable source: consumed before the call returns
+    }
+    P2G_TRY(ctx->recs2.ensure(static_cast<size_t>(kPanel) * m * 64 + kPanel * kPanel * 64));
+    uint32_t *recsA = ctx->recs2.as<uint32_t>();
+    uint32_t *recsO = recsA + kPanel * kPanel * 16;
+    for (int c0 = 0; c0 < m; c0 += kPanel) {
+        const int b = std::min(kPanel, m - c0);
+        gj_panel<<<1, kGjThreads, 0, ctx->stream>>>(M, m, W, c0, b, pb, status, ctx->d_log,
+                                                    ctx->d_exp);
+        P2G_CUDA(cudaGetLastError());
+        ++ctx->launches;
+        P2G_TRY(records_from_matrix(ctx, pb.akk_inv, b, b, recsA));
+        const int no = m - b;
+        if (no > 0) {
+            size_t n = static_cast<size_t>(b) * no;
+            gj_records_rows<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx->stream>>>(
+                M, W, pb.orow, c0, b, no, recsO);
+            P2G_CUDA(cudaGetLastError());
+            ++ctx->launches;
+        }
+        P2G_TRY(muladd_run(ctx, pb.kptr, b, xptr, b, row_bytes, recsA, 0));
+        if (no > 0)
+            P2G_TRY(muladd_run(ctx, const_cast<const uint8_t *const *>(xptr), b, pb.optr, no,
+                               row_bytes, recsO, 1));
+        gj_copy_rows<<<dim3(8, b), 256, 0, ctx->stream>>>(
+            const_cast<const uint8_t *const *>(xptr), pb.kptr, b, row_bytes);
+        P2G_CUDA(cudaGetLastError());
+        ++ctx->launches;
+    }
+    gj_extract_perm<<<g, 256, 0, ctx->stream>>>(M, m, W, pb.kall, d_inv);
     P2G_CUDA(cudaGetLastError());
     ++ctx->launches;
     return P2G_OK;

@@ -24,7 +24,7 @@ def par2_matrix(k, missing, exps):
     return np.array([[oracle.gf_pow(int(c[j]), int(e)) for j in missing] for e in exps], np.uint16)
 
 
-@pytest.mark.parametrize("m", [1, 2, 13, 64, 200])
+@pytest.mark.parametrize("m", [1, 2, 13, 64, 96, 97, 130, 200, 333])
 def test_reconstruction_matrix_matches_oracle(ctx, m):
     rng = np.random.default_rng(m)
     k = 4 * m + 7
@@ -56,6 +56,33 @@ def test_invert_random_and_singular(ctx):
         ctx.invert(S)
     assert ei.value.code == par2gpu.ESINGULAR
     assert "Singular matrix" in par2gpu.last_error()
+
+
+def test_blocked_inversion_random_and_singular(ctx):
+    """Matrices above the single-CTA size go through the blocked elimination
+    (64-column panels whose row updates run on the multiply-accumulate
+    kernel); singular ones must be reported, not faulted on."""
+    import par2gpu
+
+    rng = np.random.default_rng(12)
+    for m in (100, 160, 257):
+        A = rng.integers(0, 65536, (m, m), dtype=np.uint16)
+        want = oracle.invert(A)
+        assert want is not None
+        assert np.array_equal(ctx.invert(A), want), m
+    A = rng.integers(0, 65536, (150, 150), dtype=np.uint16)
+    A[:, 70] = 0                       # a zero column in the second panel
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        ctx.invert(A)
+    assert ei.value.code == par2gpu.ESINGULAR
+    A = rng.integers(0, 65536, (200, 200), dtype=np.uint16)
+    A[150] = A[3]                      # two equal rows
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        ctx.invert(A)
+    assert ei.value.code == par2gpu.ESINGULAR
+    # the context stays usable after a singular matrix
+    B = rng.integers(0, 65536, (120, 120), dtype=np.uint16)
+    assert np.array_equal(ctx.invert(B), oracle.invert(B))
 
 
 def test_quickpar_repair_scenarios(ctx):
