@@ -61,7 +61,8 @@ int p2g_create(int device, p2g_ctx **out);
 int p2g_destroy(p2g_ctx *ctx);
 
 /* Runs the context's work on a caller-supplied CUDA stream (a cudaStream_t
- * passed as void*; NULL restores the context's own stream).  Calls still
+ * passed as void*; NULL restores the context's own non-blocking stream, so
+ * pass cudaStreamLegacy to mean the legacy default stream).  Calls still
  * return only when their work is complete.  No counterpart in par2-rs: it is
  * the device-side plumbing a host integration needs. */
 int p2g_set_stream(p2g_ctx *ctx, void *cuda_stream);
@@ -183,6 +184,57 @@ int p2g_hash_slices(p2g_ctx *ctx, const uint8_t *const *slices, size_t n, size_t
 int p2g_verify_slices(p2g_ctx *ctx, const uint8_t *const *slices, size_t n, size_t slice_bytes,
                       const uint8_t *md5_expect, const uint32_t *crc_expect, uint8_t *ok_out,
                       uint32_t flags);
+
+/* ---- batches of independent jobs ---------------------------------------
+ * Many recovery sets of uneven sizes in one execution: per phase ONE
+ * persistent kernel takes (job, column tile, output block, input split)
+ * items, longest first, from a device queue -- instead of per-set launches
+ * that leave most SMs idle for small sets.  No counterpart in par2-rs (it
+ * handles one set per process); the per-job work is that of p2g_encode,
+ * p2g_repair and p2g_verify_slices. */
+#define P2G_JOB_CREATE 1
+#define P2G_JOB_REPAIR 2
+#define P2G_JOB_VERIFY 3
+
+typedef struct {
+    int kind;                    /* P2G_JOB_* */
+    size_t k;                    /* input slices of the recovery set (fixes the constants) */
+    size_t slice_bytes;
+    size_t col_begin, col_end;   /* byte range of every slice this job covers; col_end = 0
+                                    means the whole slice; col_begin a multiple of 2048
+                                    (column ranges are independent: the work is
+                                    column-separable).  VERIFY jobs take whole slices. */
+    const uint8_t *const *src;   /* CREATE, VERIFY: k slices; REPAIR: the k - n present ones */
+    size_t n;                    /* CREATE: recovery slices; REPAIR: missing slices */
+    const uint32_t *exps;        /* CREATE, REPAIR: n exponents */
+    const uint64_t *missing;     /* REPAIR: n ascending slice indices */
+    const uint8_t *const *recovery; /* REPAIR: n recovery slices */
+    const uint16_t *inverse;     /* REPAIR: optional host n x n decode matrix
+                                    (p2g_reconstruction_matrix); NULL: computed here */
+    uint8_t *const *out;         /* CREATE, REPAIR: n output slices */
+    uint8_t *md5_out;            /* VERIFY: host, 16 bytes per slice */
+    uint32_t *crc_out;           /* VERIFY: host, one per slice */
+    int status;                  /* set by p2g_batch_run: P2G_OK, P2G_ESINGULAR, ... */
+} p2g_job;
+
+typedef struct p2g_batch p2g_batch;
+
+#define P2G_BATCH_GRAPH 0x2u /* capture the device work into a CUDA graph for replay */
+
+/* Prepares a batch: validates the jobs, computes the decode matrices of
+ * REPAIR jobs (a singular one marks that job P2G_ESINGULAR and drops it),
+ * sizes and allocates the batch's scratch, uploads its work tables and, with
+ * P2G_BATCH_GRAPH, captures the device work into a CUDA graph.  Slice
+ * pointers are device pointers; `jobs` must outlive the batch. */
+int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags,
+                     p2g_batch **out);
+/* Runs (or replays) the batch and waits for it; fills statuses and hashes. */
+int p2g_batch_run(p2g_batch *batch);
+/* Starts the batch without waiting; p2g_batch_wait completes it. */
+int p2g_batch_launch(p2g_batch *batch);
+int p2g_batch_poll(p2g_batch *batch, int *done);
+int p2g_batch_wait(p2g_batch *batch);
+int p2g_batch_destroy(p2g_batch *batch);
 
 /* Size of the fixed device scratch array behind p2g_encode_noalloc. */
 #define P2G_NOALLOC_SCRATCH_BYTES (64u << 20)

@@ -1,0 +1,719 @@
+// batch.cu -- batches of independent create / repair / verify jobs.
+//
+// Many recovery sets of uneven file sizes, slice sizes and redundancy run
+// together: every REPAIR job's decode matrix is formed first (K2), then two
+// phases of multiply-accumulate work each run as ONE persistent kernel over a
+// queue of (problem, column tile, output block, input split) items sorted
+// longest first:
+//   phase A: CREATE jobs (sources -> recovery slices) and the first REPAIR
+//            pass (RHS = recovery ^ V * present, into scratch);
+//   phase B: the second REPAIR pass (missing = A^-1 * RHS).
+// VERIFY jobs are hashed by one launch per distinct slice size.  The device
+// work can be captured once into a CUDA graph and replayed.
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "hash.cuh"
+#include "invert.cuh"
+#include "muladd.cuh"
+
+using namespace p2g;
+
+namespace {
+
+size_t al256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
+size_t al16(size_t n) { return (n + 15) & ~static_cast<size_t>(15); }
+
+// Host image of the batch's device tables, laid out with 256-byte alignment.
+struct Image {
+    std::vector<uint8_t> bytes;
+    size_t put(const void *p, size_t n)
+    {
+        const size_t off = al256(bytes.size());
+        bytes.resize(off + al256(n ? n : 1));
+        if (p && n)
+            memcpy(bytes.data() + off, p, n);
+        return off;
+    }
+};
+
+struct HashGroup {
+    size_t ptr_off;  // device table of slice pointers
+    size_t S;
+    int n;
+    size_t out_off;  // into hash buffer: md5 (n*16), then crc (n*4)
+    std::vector<std::pair<int, int>> slices;  // (job, slice index) of each entry
+};
+
+struct Phase {
+    size_t planes_off = 0, rec_off = 0, prob_off = 0, item_off = 0, zero_ptr_off = 0,
+           zero_len_off = 0;
+    int nplanes = 0, nrec = 0, nitems = 0, nzero = 0, grid = 0;
+    unsigned long long planes_total = 0, rec_total = 0;
+};
+
+}  // namespace
+
+struct p2g_batch {
+    p2g_ctx *ctx = nullptr;
+    p2g_job *jobs = nullptr;
+    size_t njobs = 0;
+    DevBuf params, hparams, planes, recs, rhs, inv, hashbuf;
+    Phase A, B;
+    size_t copy_src_off = 0, copy_dst_off = 0, copy_len_off = 0, counter_off = 0;
+    int ncopy = 0;
+    std::vector<HashGroup> hash;
+    DevBuf hash_host;  // pinned
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done = nullptr;
+    bool launched = false;
+};
+
+namespace {
+
+uint8_t *dp(p2g_batch *b, size_t off) { return b->params.as<uint8_t>() + off; }
+
+int enqueue(p2g_batch *b)
+{
+    p2g_ctx *ctx = b->ctx;
+    cudaStream_t st = ctx->stream;
+    P2G_CUDA(cudaMemsetAsync(dp(b, b->counter_off), 0, 2 * sizeof(int), st));
+    P2G_TRY(batch_copy(st, reinterpret_cast<const uint8_t *const *>(dp(b, b->copy_src_off)),
+                       reinterpret_cast<uint8_t *const *>(dp(b, b->copy_dst_off)),
+                       reinterpret_cast<const unsigned long long *>(dp(b, b->copy_len_off)),
+                       b->ncopy));
+    Phase *ph[2] = {&b->A, &b->B};
+    for (int x = 0; x < 2; ++x) {
+        Phase &P = *ph[x];
+        if (!P.nitems)
+            continue;
+        P2G_TRY(batch_planes(st, reinterpret_cast<const PlanesProb *>(dp(b, P.planes_off)),
+                             P.nplanes, P.planes_total));
+        P2G_TRY(batch_records(st, ctx->d_log, ctx->d_exp,
+                              reinterpret_cast<const RecProb *>(dp(b, P.rec_off)), P.nrec,
+                              P.rec_total));
+        P2G_TRY(batch_zero(st, reinterpret_cast<uint8_t *const *>(dp(b, P.zero_ptr_off)),
+                           reinterpret_cast<const unsigned long long *>(dp(b, P.zero_len_off)),
+                           P.nzero));
+        if (x == 0)
+            ctx->mark(2);
+        P2G_TRY(batch_muladd(st, P.grid, reinterpret_cast<const BatchProb *>(dp(b, P.prob_off)),
+                             reinterpret_cast<const BatchItem *>(dp(b, P.item_off)), P.nitems,
+                             reinterpret_cast<int *>(dp(b, b->counter_off)) + x));
+        ctx->launches += 4;
+    }
+    ctx->mark(3);
+    for (const HashGroup &g : b->hash) {
+        uint8_t *out = b->hashbuf.as<uint8_t>() + g.out_off;
+        P2G_TRY(hash_run(ctx, reinterpret_cast<const uint8_t *const *>(dp(b, g.ptr_off)), g.n, g.S,
+                         out, reinterpret_cast<uint32_t *>(out + al16(static_cast<size_t>(g.n) * 16))));
+    }
+    return P2G_OK;
+}
+
+// Per-problem description gathered while scanning the jobs.
+struct Prob {
+    int phase;
+    size_t src_off, dst_off;        // param offsets of the pointer arrays
+    int nin, nout;
+    size_t S;
+    int mode;
+    // records: par2 (consts/exps offsets) or matrix (coeff device pointer)
+    size_t consts_off, exps_off;
+    const uint16_t *coeff;  // device
+};
+
+}  // namespace
+
+extern "C" {
+
+int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, p2g_batch **out)
+{
+    clear_error();
+    if (!ctx || !out || (njobs && !jobs)) {
+        set_error("p2g_batch_create: null argument");
+        return P2G_EINVAL;
+    }
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    ctx->launches = 0;
+    for (bool &m : ctx->ev_marked)
+        m = false;
+    // ---- validation ----
+    for (size_t j = 0; j < njobs; ++j) {
+        p2g_job &J = jobs[j];
+        J.status = P2G_OK;
+        const size_t cb = J.col_begin, ce = J.col_end ? J.col_end : J.slice_bytes;
+        bool bad = J.slice_bytes == 0 || J.slice_bytes % 2 || cb % 2048 || ce > J.slice_bytes ||
+                   cb >= ce || ce % 2 || J.k == 0 || J.k > 65535 || !J.src;
+        if (J.kind == P2G_JOB_CREATE)
+            bad = bad || J.n > 65535 || (J.n && (!J.exps || !J.out));
+        else if (J.kind == P2G_JOB_REPAIR)
+            bad = bad || J.n == 0 || J.n > J.k || !J.exps || !J.missing || !J.recovery || !J.out;
+        else if (J.kind == P2G_JOB_VERIFY)
+            bad = bad || cb != 0 || ce != J.slice_bytes || !J.md5_out || !J.crc_out;
+        else
+            bad = true;
+        if (J.kind == P2G_JOB_REPAIR && !bad)
+            for (size_t q = 0; q < J.n; ++q)
+                bad = bad || J.missing[q] >= J.k || (q && J.missing[q] <= J.missing[q - 1]);
+        if (bad) {
+            set_error("p2g_batch_create: job %zu is malformed", j);
+            return P2G_EINVAL;
+        }
+        // the kernels move 16-byte vectors: every slice must start 16-byte aligned
+        auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+        bool aligned = true;
+        const size_t nsrc = J.kind == P2G_JOB_REPAIR ? J.k - J.n : J.k;
+        for (size_t i = 0; i < nsrc; ++i)
+            aligned = aligned && J.src[i] && al(J.src[i]);
+        if (J.kind != P2G_JOB_VERIFY)
+            for (size_t e = 0; e < J.n; ++e)
+                aligned = aligned && J.out[e] && al(J.out[e]) &&
+                          (J.kind != P2G_JOB_REPAIR || (J.recovery[e] && al(J.recovery[e])));
+        if (!aligned) {
+            set_error("p2g_batch_create: job %zu has a null or non-16-byte-aligned slice pointer",
+                      j);
+            return P2G_EINVAL;
+        }
+    }
+    p2g_batch *b = new p2g_batch();
+    b->ctx = ctx;
+    b->jobs = jobs;
+    b->njobs = njobs;
+    b->hparams.pinned = true;
+    b->hash_host.pinned = true;
+    auto fail = [&](int rc) {
+        p2g_batch_destroy(b);
+        return rc;
+    };
+    // ---- decode matrices of REPAIR jobs ----
+    std::vector<size_t> inv_off(njobs, 0);
+    size_t inv_bytes = 0;
+    for (size_t j = 0; j < njobs; ++j)
+        if (jobs[j].kind == P2G_JOB_REPAIR) {
+            inv_off[j] = inv_bytes;
+            inv_bytes += al256(jobs[j].n * jobs[j].n * 2);
+        }
+    if (int rc = b->inv.ensure(inv_bytes + 256))
+        return fail(rc);
+    std::vector<int> singular(njobs, 0);
+    {
+        std::vector<int> pending;
+        DevBuf stat;
+        if (int rc = stat.ensure(njobs * sizeof(int) + 16))
+            return fail(rc);
+        std::vector<uint8_t> h;
+        for (size_t j = 0; j < njobs; ++j) {
+            p2g_job &J = jobs[j];
+            if (J.kind != P2G_JOB_REPAIR)
+                continue;
+            uint16_t *d_inv = reinterpret_cast<uint16_t *>(b->inv.as<uint8_t>() + inv_off[j]);
+            if (J.inverse) {
+                if (cudaMemcpyAsync(d_inv, J.inverse, J.n * J.n * 2, cudaMemcpyHostToDevice,
+                                    ctx->stream) != cudaSuccess) {
+                    set_error("p2g_batch_create: decode matrix upload failed");
+                    stat.release();
+                    return fail(P2G_ECUDA);
+                }
+                continue;
+            }
+            // constants of the missing slices and the exponents
+            std::vector<uint16_t> c(J.k);
+            par2_constants(J.k, c.data());
+            const size_t m = J.n;
+            h.assign(al256(m * 2) + m * 4, 0);
+            for (size_t q = 0; q < m; ++q)
+                reinterpret_cast<uint16_t *>(h.data())[q] = c[J.missing[q]];
+            memcpy(h.data() + al256(m * 2), J.exps, m * 4);
+            int rc = ctx->coeffs.ensure(h.size() + 16);
+            if (rc == P2G_OK &&
+                cudaMemcpyAsync(ctx->coeffs.p, h.data(), h.size(), cudaMemcpyHostToDevice,
+                                ctx->stream) != cudaSuccess)
+                rc = P2G_ECUDA;
+            GjWork w{ctx->gj_M, ctx->gj_status};
+            if (rc == P2G_OK)
+                rc = gj_invert(ctx, w, static_cast<int>(m), ctx->coeffs.as<uint16_t>(),
+                               reinterpret_cast<const uint32_t *>(ctx->coeffs.as<uint8_t>() +
+                                                                  al256(m * 2)),
+                               nullptr, d_inv);
+            if (rc == P2G_OK &&
+                cudaMemcpyAsync(stat.as<int>() + j, ctx->gj_status.p, sizeof(int),
+                                cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+                rc = P2G_ECUDA;
+            // the pageable host source is consumed before the next iteration
+            // reuses `h`, and ctx->coeffs before the next upload (stream order)
+            if (rc != P2G_OK) {
+                stat.release();
+                return fail(rc);
+            }
+            pending.push_back(static_cast<int>(j));
+        }
+        if (!pending.empty()) {
+            std::vector<int> st(njobs, 0);
+            if (cudaMemcpyAsync(st.data(), stat.p, njobs * sizeof(int), cudaMemcpyDeviceToHost,
+                                ctx->stream) != cudaSuccess ||
+                cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+                set_error("p2g_batch_create: inversion failed: %s",
+                          cudaGetErrorString(cudaGetLastError()));
+                stat.release();
+                return fail(P2G_ECUDA);
+            }
+            for (int j : pending)
+                if (st[j]) {
+                    singular[j] = 1;
+                    jobs[j].status = P2G_ESINGULAR;
+                }
+        }
+        stat.release();
+    }
+    // ---- problems ----
+    Image img;
+    std::vector<Prob> probs;
+    std::vector<uint8_t *> copy_src, copy_dst;
+    std::vector<unsigned long long> copy_len;
+    size_t rhs_bytes = 0;
+    std::vector<size_t> rhs_off(njobs, 0);
+    for (size_t j = 0; j < njobs; ++j)
+        if (jobs[j].kind == P2G_JOB_REPAIR && !singular[j]) {
+            const size_t S = (jobs[j].col_end ? jobs[j].col_end : jobs[j].slice_bytes) - jobs[j].col_begin;
+            rhs_off[j] = rhs_bytes;
+            rhs_bytes += al256(jobs[j].n * al16(S));
+        }
+    if (int rc = b->rhs.ensure(rhs_bytes + 256))
+        return fail(rc);
+    std::vector<HashGroup> hg;
+    for (size_t j = 0; j < njobs; ++j) {
+        p2g_job &J = jobs[j];
+        const size_t cb = J.col_begin;
+        const size_t S = (J.col_end ? J.col_end : J.slice_bytes) - cb;
+        if (J.kind == P2G_JOB_VERIFY) {
+            HashGroup *g = nullptr;
+            for (HashGroup &x : hg)
+                if (x.S == S)
+                    g = &x;
+            if (!g) {
+                hg.push_back(HashGroup());
+                g = &hg.back();
+                g->S = S;
+                g->n = 0;
+            }
+            for (size_t i = 0; i < J.k; ++i)
+                g->slices.push_back({static_cast<int>(j), static_cast<int>(i)});
+            continue;
+        }
+        if (J.kind == P2G_JOB_CREATE) {
+            if (J.n == 0)
+                continue;
+            std::vector<const uint8_t *> s(J.k);
+            std::vector<uint8_t *> d(J.n);
+            for (size_t i = 0; i < J.k; ++i)
+                s[i] = J.src[i] + cb;
+            for (size_t e = 0; e < J.n; ++e)
+                d[e] = J.out[e] + cb;
+            std::vector<uint16_t> c(J.k);
+            par2_constants(J.k, c.data());
+            Prob p{};
+            p.phase = 0;
+            p.src_off = img.put(s.data(), s.size() * sizeof(void *));
+            p.dst_off = img.put(d.data(), d.size() * sizeof(void *));
+            p.consts_off = img.put(c.data(), c.size() * 2);
+            p.exps_off = img.put(J.exps, J.n * 4);
+            p.nin = static_cast<int>(J.k);
+            p.nout = static_cast<int>(J.n);
+            p.S = S;
+            p.mode = 0;
+            probs.push_back(p);
+            continue;
+        }
+        // REPAIR
+        if (singular[j])
+            continue;
+        const size_t m = J.n, np = J.k - m;
+        std::vector<uint16_t> c(J.k), cp;
+        par2_constants(J.k, c.data());
+        {
+            size_t q = 0;
+            for (size_t i = 0; i < J.k; ++i) {
+                if (q < m && J.missing[q] == i)
+                    ++q;
+                else
+                    cp.push_back(c[i]);
+            }
+        }
+        std::vector<uint8_t *> rh(m), o(m);
+        for (size_t q = 0; q < m; ++q) {
+            rh[q] = b->rhs.as<uint8_t>() + rhs_off[j] + q * al16(S);
+            o[q] = J.out[q] + cb;
+            copy_src.push_back(const_cast<uint8_t *>(J.recovery[q]) + cb);
+            copy_dst.push_back(rh[q]);
+            copy_len.push_back(S);
+        }
+        const size_t rh_off = img.put(rh.data(), m * sizeof(void *));
+        if (np) {
+            std::vector<const uint8_t *> s(np);
+            for (size_t i = 0; i < np; ++i)
+                s[i] = J.src[i] + cb;
+            Prob p{};
+            p.phase = 0;
+            p.src_off = img.put(s.data(), np * sizeof(void *));
+            p.dst_off = rh_off;
+            p.consts_off = img.put(cp.data(), np * 2);
+            p.exps_off = img.put(J.exps, m * 4);
+            p.nin = static_cast<int>(np);
+            p.nout = static_cast<int>(m);
+            p.S = S;
+            p.mode = 1;
+            probs.push_back(p);
+        }
+        Prob p{};
+        p.phase = 1;
+        p.src_off = rh_off;
+        p.dst_off = img.put(o.data(), m * sizeof(void *));
+        p.coeff = reinterpret_cast<const uint16_t *>(b->inv.as<uint8_t>() + inv_off[j]);
+        p.nin = static_cast<int>(m);
+        p.nout = static_cast<int>(m);
+        p.S = S;
+        p.mode = 0;
+        probs.push_back(p);
+    }
+    // ---- scratch and work tables per phase ----
+    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    size_t plane_need = 0, rec_need = 0;
+    for (int x = 0; x < 2; ++x) {
+        size_t pl = 0, rc = 0;
+        for (const Prob &p : probs)
+            if (p.phase == x) {
+                pl += static_cast<size_t>(p.nin) * ((p.S + 2047) / 2048) * 2048;
+                rc += static_cast<size_t>(p.nin) * p.nout * 64;
+            }
+        plane_need = std::max(plane_need, pl);
+        rec_need = std::max(rec_need, rc);
+    }
+    if (int rc = b->planes.ensure(plane_need + 256))
+        return fail(rc);
+    if (int rc = b->recs.ensure(rec_need + 256))
+        return fail(rc);
+    b->copy_src_off = img.put(copy_src.data(), copy_src.size() * sizeof(void *));
+    b->copy_dst_off = img.put(copy_dst.data(), copy_dst.size() * sizeof(void *));
+    b->copy_len_off = img.put(copy_len.data(), copy_len.size() * 8);
+    b->ncopy = static_cast<int>(copy_src.size());
+    b->counter_off = img.put(nullptr, 2 * sizeof(int));
+    // The device addresses of the image are only known after the upload
+    // buffer exists: size it first (tables below reference image offsets).
+    struct Pending {
+        std::vector<PlanesProb> pl;
+        std::vector<RecProb> rc;
+        std::vector<BatchProb> bp;
+        std::vector<BatchItem> items;
+        std::vector<uint8_t *> zptr;
+        std::vector<unsigned long long> zlen;
+    } ph[2];
+    // the params buffer must exist before pointers into it are formed: the
+    // image grows below, so reserve generously and fix the base afterwards
+    std::vector<std::pair<size_t, int>> fixups;  // (image offset of a pointer field, kind)
+    for (int x = 0; x < 2; ++x) {
+        Pending &P = ph[x];
+        size_t pl_off = 0, rc_off = 0;
+        unsigned long long pl_first = 0, rc_first = 0;
+        double total_cost = 0;
+        for (const Prob &p : probs)
+            if (p.phase == x)
+                total_cost += static_cast<double>(p.nin) * ((p.S + 2047) / 2048) *
+                              ((p.nout + kBatchBlock - 1) / kBatchBlock) *
+                              (512.0 + 32.0 * std::min(p.nout, kBatchBlock));
+        const double target = std::max(1.0, total_cost / (4.0 * sms));
+        for (size_t pi = 0; pi < probs.size(); ++pi) {
+            const Prob &p = probs[pi];
+            if (p.phase != x)
+                continue;
+            const int T = static_cast<int>((p.S + 2047) / 2048);
+            PlanesProb pp{};
+            pp.S = p.S;
+            pp.nin = p.nin;
+            pp.T = T;
+            pp.first = pl_first;
+            // pointer fields hold image offsets for now; rebased after upload
+            pp.src = reinterpret_cast<const uint8_t *const *>(p.src_off);
+            pp.planes = reinterpret_cast<uint32_t *>(b->planes.as<uint8_t>() + pl_off);
+            P.pl.push_back(pp);
+            RecProb rp{};
+            rp.nin = p.nin;
+            rp.nout = p.nout;
+            rp.first = rc_first;
+            rp.coeff = p.coeff;
+            rp.consts = p.coeff ? nullptr : reinterpret_cast<const uint16_t *>(p.consts_off);
+            rp.exps = p.coeff ? nullptr : reinterpret_cast<const uint32_t *>(p.exps_off);
+            rp.recs = reinterpret_cast<uint32_t *>(b->recs.as<uint8_t>() + rc_off);
+            P.rc.push_back(rp);
+            BatchProb bp{};
+            bp.planes = pp.planes;
+            bp.recs = rp.recs;
+            bp.dst = reinterpret_cast<uint8_t *const *>(p.dst_off);
+            bp.S = p.S;
+            bp.nin = p.nin;
+            bp.nout = p.nout;
+            bp.T = T;
+            bp.nblk = (p.nout + kBatchBlock - 1) / kBatchBlock;
+            bp.mode = p.mode;
+            const double unit = static_cast<double>(p.nin) *
+                                (512.0 + 32.0 * std::min(p.nout, kBatchBlock));
+            int ns = 1;
+            if (unit > target && p.S % 4 == 0)
+                ns = static_cast<int>(std::min<double>({std::ceil(unit / target),
+                                                        std::max(1.0, p.nin / 16.0), 64.0}));
+            bp.nsplit = std::max(1, ns);
+            const int bpi = static_cast<int>(P.bp.size());
+            P.bp.push_back(bp);
+            for (int t = 0; t < T; ++t)
+                for (int ob = 0; ob < bp.nblk; ++ob)
+                    for (int sp = 0; sp < bp.nsplit; ++sp)
+                        P.items.push_back(BatchItem{bpi, t, ob, sp});
+            if (bp.nsplit > 1 && bp.mode == 0) {
+                // outputs are folded with atomic XOR: start them at zero
+                for (int e = 0; e < p.nout; ++e) {
+                    uint8_t *ptr;
+                    memcpy(&ptr, img.bytes.data() + p.dst_off + e * sizeof(void *), sizeof ptr);
+                    P.zptr.push_back(ptr);
+                    P.zlen.push_back(p.S);
+                }
+            }
+            pl_off += static_cast<size_t>(p.nin) * T * 2048;
+            rc_off += static_cast<size_t>(p.nin) * p.nout * 64;
+            pl_first += static_cast<unsigned long long>(p.nin) * T * 32;
+            rc_first += static_cast<unsigned long long>(p.nin) * p.nout;
+        }
+        // longest items first
+        std::vector<double> cost(P.items.size());
+        for (size_t i = 0; i < P.items.size(); ++i) {
+            const BatchItem &it = P.items[i];
+            const BatchProb &bp = P.bp[it.prob];
+            const int nb = std::min(kBatchBlock, bp.nout - it.ob * kBatchBlock);
+            cost[i] = static_cast<double>(bp.nin) / bp.nsplit * (512.0 + 32.0 * nb);
+        }
+        std::vector<size_t> order(P.items.size());
+        for (size_t i = 0; i < order.size(); ++i)
+            order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t a, size_t c) { return cost[a] > cost[c]; });
+        std::vector<BatchItem> sorted(order.size());
+        for (size_t i = 0; i < order.size(); ++i)
+            sorted[i] = P.items[order[i]];
+        P.items.swap(sorted);
+        Phase &D = x == 0 ? b->A : b->B;
+        D.nplanes = static_cast<int>(P.pl.size());
+        D.nrec = static_cast<int>(P.rc.size());
+        D.nitems = static_cast<int>(P.items.size());
+        D.nzero = static_cast<int>(P.zptr.size());
+        D.grid = std::min(D.nitems, sms);
+        D.planes_total = pl_first;
+        D.rec_total = rc_first;
+    }
+    // tables go at the end of the image; pointer fields that hold image
+    // offsets are rebased to device addresses once the buffer exists
+    for (int x = 0; x < 2; ++x) {
+        Phase &D = x == 0 ? b->A : b->B;
+        D.planes_off = img.put(nullptr, ph[x].pl.size() * sizeof(PlanesProb));
+        D.rec_off = img.put(nullptr, ph[x].rc.size() * sizeof(RecProb));
+        D.prob_off = img.put(nullptr, ph[x].bp.size() * sizeof(BatchProb));
+        D.item_off = img.put(ph[x].items.data(), ph[x].items.size() * sizeof(BatchItem));
+        D.zero_ptr_off = img.put(ph[x].zptr.data(), ph[x].zptr.size() * sizeof(void *));
+        D.zero_len_off = img.put(ph[x].zlen.data(), ph[x].zlen.size() * 8);
+    }
+    for (HashGroup &g : hg) {
+        g.n = static_cast<int>(g.slices.size());
+        std::vector<const uint8_t *> ptrs(g.n);
+        for (int i = 0; i < g.n; ++i)
+            ptrs[i] = jobs[g.slices[i].first].src[g.slices[i].second];
+        g.ptr_off = img.put(ptrs.data(), ptrs.size() * sizeof(void *));
+    }
+    if (int rc = b->params.ensure(img.bytes.size() + 256))
+        return fail(rc);
+    uint8_t *base = b->params.as<uint8_t>();
+    auto rebase = [&](const void *off) { return base + reinterpret_cast<uintptr_t>(off); };
+    for (int x = 0; x < 2; ++x) {
+        Phase &D = x == 0 ? b->A : b->B;
+        for (PlanesProb &q : ph[x].pl)
+            q.src = reinterpret_cast<const uint8_t *const *>(rebase(q.src));
+        for (RecProb &q : ph[x].rc) {
+            if (!q.coeff) {
+                q.consts = reinterpret_cast<const uint16_t *>(rebase(q.consts));
+                q.exps = reinterpret_cast<const uint32_t *>(rebase(q.exps));
+            }
+        }
+        for (BatchProb &q : ph[x].bp)
+            q.dst = reinterpret_cast<uint8_t *const *>(rebase(q.dst));
+        memcpy(img.bytes.data() + D.planes_off, ph[x].pl.data(), ph[x].pl.size() * sizeof(PlanesProb));
+        memcpy(img.bytes.data() + D.rec_off, ph[x].rc.data(), ph[x].rc.size() * sizeof(RecProb));
+        memcpy(img.bytes.data() + D.prob_off, ph[x].bp.data(), ph[x].bp.size() * sizeof(BatchProb));
+    }
+    // verify outputs
+    size_t hbytes = 0;
+    for (HashGroup &g : hg) {
+        g.out_off = hbytes;
+        hbytes += al256(al16(static_cast<size_t>(g.n) * 16) + static_cast<size_t>(g.n) * 4);
+    }
+    if (int rc = b->hashbuf.ensure(hbytes + 256))
+        return fail(rc);
+    if (hbytes)
+        if (int rc = b->hash_host.ensure(hbytes + 256))
+            return fail(rc);
+    b->hash = hg;
+    if (int rc = b->hparams.ensure(img.bytes.size() + 256))
+        return fail(rc);
+    memcpy(b->hparams.p, img.bytes.data(), img.bytes.size());
+    if (cudaMemcpyAsync(b->params.p, b->hparams.p, img.bytes.size(), cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) {
+        set_error("p2g_batch_create: table upload failed");
+        return fail(P2G_ECUDA);
+    }
+    if (flags & P2G_BATCH_GRAPH) {
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            set_error("p2g_batch_create: %s", cudaGetErrorString(cudaGetLastError()));
+            return fail(P2G_ECUDA);
+        }
+        const bool timing = ctx->timing;
+        ctx->timing = false;  // no event records inside the graph
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        int rc = e == cudaSuccess ? enqueue(b) : P2G_ECUDA;
+        cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &b->graph);
+        ctx->timing = timing;
+        if (rc != P2G_OK || e2 != cudaSuccess ||
+            cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
+            (void)cudaGetLastError();
+            set_error("p2g_batch_create: graph capture failed");
+            return fail(rc != P2G_OK ? rc : P2G_ECUDA);
+        }
+    }
+    *out = b;
+    return P2G_OK;
+}
+
+int p2g_batch_launch(p2g_batch *b)
+{
+    clear_error();
+    if (!b) {
+        set_error("p2g_batch_launch: null batch");
+        return P2G_EINVAL;
+    }
+    p2g_ctx *ctx = b->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    ctx->launches = 0;
+    for (bool &m : ctx->ev_marked)
+        m = false;
+    ctx->mark(0);
+    if (b->exec) {
+        P2G_CUDA(cudaGraphLaunch(b->exec, ctx->stream));
+        ctx->launches = 1;
+    } else {
+        P2G_TRY(enqueue(b));
+    }
+    if (b->hash_host.p)
+        P2G_CUDA(cudaMemcpyAsync(b->hash_host.p, b->hashbuf.p, b->hash_host.cap,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->mark(4);
+    P2G_CUDA(cudaEventRecord(b->done, ctx->stream));
+    b->launched = true;
+    return P2G_OK;
+}
+
+int p2g_batch_poll(p2g_batch *b, int *done)
+{
+    clear_error();
+    if (!b || !done) {
+        set_error("p2g_batch_poll: null argument");
+        return P2G_EINVAL;
+    }
+    cudaError_t e = cudaEventQuery(b->done);
+    if (e == cudaErrorNotReady) {
+        (void)cudaGetLastError();
+        *done = 0;
+        return P2G_OK;
+    }
+    P2G_CUDA(e);
+    *done = 1;
+    return P2G_OK;
+}
+
+int p2g_batch_wait(p2g_batch *b)
+{
+    clear_error();
+    if (!b || !b->launched) {
+        set_error("p2g_batch_wait: batch not launched");
+        return P2G_EINVAL;
+    }
+    p2g_ctx *ctx = b->ctx;
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    P2G_CUDA(cudaEventSynchronize(b->done));
+    P2G_CUDA(cudaGetLastError());
+    b->launched = false;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        ctx->last = p2g_timing{};
+        ctx->last.launches = ctx->launches;
+        if (ctx->timing) {
+            auto el = [&](int a, int c) {
+                float ms = 0.f;
+                if (ctx->ev_marked[a] && ctx->ev_marked[c])
+                    cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[c]);
+                return ms;
+            };
+            ctx->last.ms_kernel = el(2, 3);
+            ctx->last.ms_total = el(0, 4);
+        }
+    }
+    for (const HashGroup &g : b->hash) {
+        const uint8_t *md5 = b->hash_host.as<uint8_t>() + g.out_off;
+        const uint32_t *crc = reinterpret_cast<const uint32_t *>(md5 + al16(static_cast<size_t>(g.n) * 16));
+        for (int i = 0; i < g.n; ++i) {
+            p2g_job &J = b->jobs[g.slices[i].first];
+            const int s = g.slices[i].second;
+            memcpy(J.md5_out + 16 * s, md5 + 16 * i, 16);
+            J.crc_out[s] = crc[i];
+        }
+    }
+    return P2G_OK;
+}
+
+int p2g_batch_run(p2g_batch *b)
+{
+    P2G_TRY(p2g_batch_launch(b));
+    return p2g_batch_wait(b);
+}
+
+int p2g_batch_destroy(p2g_batch *b)
+{
+    if (!b)
+        return P2G_OK;
+    if (b->ctx) {
+        cudaSetDevice(b->ctx->device);
+        if (b->launched && b->done)
+            cudaEventSynchronize(b->done);
+    }
+    if (b->exec)
+        cudaGraphExecDestroy(b->exec);
+    if (b->graph)
+        cudaGraphDestroy(b->graph);
+    if (b->done)
+        cudaEventDestroy(b->done);
+    b->params.release();
+    b->hparams.release();
+    b->planes.release();
+    b->recs.release();
+    b->rhs.release();
+    b->inv.release();
+    b->hashbuf.release();
+    b->hash_host.release();
+    delete b;
+    return P2G_OK;
+}
+
+}  // extern "C"

@@ -85,7 +85,7 @@ static const HostTables &tables()
     return t;
 }
 
-static void par2_constants(size_t k, uint16_t *out)
+void par2_constants(size_t k, uint16_t *out)
 {
     const HostTables &t = tables();
     size_t have = 0;

@@ -17,6 +17,9 @@ namespace p2g {
 void set_error(const char *fmt, ...);
 void clear_error();
 
+// PAR2 input-slice constants (par2_rs.rs:64-76) on the host.
+void par2_constants(size_t k, uint16_t *out);
+
 // Growable device (or pinned host) buffer owned by a context.
 struct DevBuf {
     void *p = nullptr;

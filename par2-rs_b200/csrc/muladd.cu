@@ -209,35 +209,32 @@ __global__ void records_par2_kernel(const uint16_t *__restrict__ consts,
 // WARPS warps per CTA; each output group of EREG outputs is held by PSPLIT
 // warps, each keeping 16 / PSPLIT of the 16 planes (PSPLIT = 2 doubles the
 // warps per SM at the same number of outputs per table).
+// One work item: column tile t, output block ob, inputs [i0, i1).  smode:
+// 0 store, 1 XOR into the outputs, 2 atomic XOR (input ranges of one tile
+// and block handled by several CTAs).
 template <int WARPS, int EREG, int PSPLIT>
-__global__ void __launch_bounds__(WARPS * 32, 1)
-    muladd_bitsliced(const uint32_t *__restrict__ planes, const uint32_t *__restrict__ recs,
-                     int nin, int nout, int T, int nblk, int nsplit,
-                     uint8_t *const *__restrict__ dst, size_t S, int mode)
+__device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__restrict__ planes,
+                                            const uint32_t *__restrict__ recs, int nin, int nout,
+                                            int T, int t, int ob, int i0, int i1,
+                                            uint8_t *const *__restrict__ dst, size_t S, int smode)
 {
     constexpr int THREADS = WARPS * 32;
     constexpr int GROUPS = WARPS / PSPLIT;   // output groups
     constexpr int NPL = 16 / PSPLIT;         // planes per warp
     constexpr int EBLK = GROUPS * EREG;
     constexpr int SLOT = kTileBytes + EBLK * 64;
-    extern __shared__ __align__(128) uint8_t smem[];
     uint32_t *tab = reinterpret_cast<uint32_t *>(smem);
     uint8_t *ring = smem + 2 * kTableBytes;
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    int bid = blockIdx.x;
-    const int split = bid % nsplit;
-    bid /= nsplit;
-    const int ob = bid % nblk;
-    const int t = bid / nblk;
     const int obase = ob * EBLK;
     const int nb = min(EBLK, nout - obase);
-    const int i0 = static_cast<int>(static_cast<long long>(nin) * split / nsplit);
-    const int i1 = static_cast<int>(static_cast<long long>(nin) * (split + 1) / nsplit);
     const int ph = warp % PSPLIT;            // which planes: [ph*NPL, ph*NPL + NPL)
-    const int my0 = (warp / PSPLIT) * EREG;
-    const int myn = max(0, min(EREG, nb - my0));
+    // a partial block's outputs are spread evenly over the groups
+    const int per = (nb + GROUPS - 1) / GROUPS;
+    const int my0 = (warp / PSPLIT) * per;
+    const int myn = max(0, min(per, nb - my0));
 
     auto issue = [&](int i) {
         if (i < i1) {
@@ -361,7 +358,6 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     }
     cp_async_wait<0>();
 
-    const int smode = nsplit > 1 ? 2 : mode;
     if constexpr (PSPLIT == 1) {
 #pragma unroll
         for (int e = 0; e < EREG; ++e) {
@@ -399,6 +395,53 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
                             static_cast<size_t>(t) * kTileBytes + lane * 64, x, smode);
             }
         }
+    }
+}
+
+template <int WARPS, int EREG, int PSPLIT>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+    muladd_bitsliced(const uint32_t *__restrict__ planes, const uint32_t *__restrict__ recs,
+                     int nin, int nout, int T, int nblk, int nsplit,
+                     uint8_t *const *__restrict__ dst, size_t S, int mode)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    int bid = blockIdx.x;
+    const int split = bid % nsplit;
+    bid /= nsplit;
+    const int ob = bid % nblk;
+    const int t = bid / nblk;
+    const int i0 = static_cast<int>(static_cast<long long>(nin) * split / nsplit);
+    const int i1 = static_cast<int>(static_cast<long long>(nin) * (split + 1) / nsplit);
+    muladd_item<WARPS, EREG, PSPLIT>(smem, planes, recs, nin, nout, T, t, ob, i0, i1, dst, S,
+                                     nsplit > 1 ? 2 : mode);
+}
+
+// Persistent form for batches of independent problems: one CTA per SM takes
+// items (problem, tile, output block, input split) from a queue ordered
+// longest first and runs each as muladd_bitsliced would.
+template <int WARPS, int EREG, int PSPLIT>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+    muladd_persistent(const BatchProb *__restrict__ probs, const BatchItem *__restrict__ items,
+                      int nitems, int *__restrict__ counter)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ int cur;
+    while (true) {
+        if (threadIdx.x == 0)
+            cur = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = cur;
+        if (it >= nitems)
+            break;
+        const BatchItem item = items[it];
+        const BatchProb p = probs[item.prob];
+        const int i0 = static_cast<int>(static_cast<long long>(p.nin) * item.split / p.nsplit);
+        const int i1 =
+            static_cast<int>(static_cast<long long>(p.nin) * (item.split + 1) / p.nsplit);
+        muladd_item<WARPS, EREG, PSPLIT>(smem, p.planes, p.recs, p.nin, p.nout, p.T, item.t,
+                                         item.ob, i0, i1, p.dst, p.S,
+                                         p.nsplit > 1 ? 2 : p.mode);
+        __syncthreads();
     }
 }
 
@@ -739,6 +782,166 @@ int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdP
     *best = best_p;
     *best_ms = best_t;
     *tried = static_cast<int>(cands.size());
+    return P2G_OK;
+}
+
+// ---- batches of independent problems -----------------------------------
+
+template <class P>
+__device__ __forceinline__ int find_prob(const P *probs, int np, unsigned long long gid)
+{
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (probs[mid].first <= gid)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void batch_planes_kernel(const PlanesProb *__restrict__ probs, int np,
+                                    unsigned long long total)
+{
+    const unsigned long long gid = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gid >= total)
+        return;
+    const PlanesProb p = probs[find_prob(probs, np, gid)];
+    const unsigned long long local = gid - p.first;
+    const int lane = static_cast<int>(local & 31);
+    const unsigned long long it = local >> 5;
+    const int t = static_cast<int>(it % p.T);
+    const int i = static_cast<int>(it / p.T);
+    uint32_t x[16];
+    load_group(p.src[i], p.S, static_cast<size_t>(t) * kTileBytes + lane * 64, x);
+    transpose16x2(x);
+    uint32_t *P = p.planes + it * 512 + lane;
+#pragma unroll
+    for (int b = 0; b < 16; ++b)
+        P[b * 32] = x[b];
+}
+
+__global__ void batch_records_kernel(const RecProb *__restrict__ probs, int np,
+                                     unsigned long long total, const uint16_t *__restrict__ glog,
+                                     const uint16_t *__restrict__ gexp)
+{
+    const unsigned long long gid = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gid >= total)
+        return;
+    const RecProb p = probs[find_prob(probs, np, gid)];
+    const unsigned long long local = gid - p.first;
+    const int o = static_cast<int>(local % p.nout);
+    const int i = static_cast<int>(local / p.nout);
+    uint32_t c;
+    if (p.coeff) {
+        c = p.coeff[static_cast<size_t>(o) * p.nin + i];
+    } else {
+        const uint32_t base = p.consts[i], e = p.exps[o];
+        if (base == 0)
+            c = e == 0 ? 1u : 0u;
+        else if (e == 0)
+            c = 1u;
+        else
+            c = gexp[static_cast<uint32_t>((static_cast<uint64_t>(glog[base]) * e) % 65535u)];
+    }
+    put_record(p.recs, local, c);
+}
+
+__global__ void batch_zero_kernel(uint8_t *const *__restrict__ ptrs,
+                                  const unsigned long long *__restrict__ bytes, int n)
+{
+    for (int j = blockIdx.y; j < n; j += gridDim.y) {
+        uint8_t *d = ptrs[j];
+        const size_t S = bytes[j];
+        for (size_t x = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 16; x < S;
+             x += static_cast<size_t>(gridDim.x) * blockDim.x * 16) {
+            if (x + 16 <= S)
+                *reinterpret_cast<uint4 *>(d + x) = make_uint4(0, 0, 0, 0);
+            else
+                for (size_t y = x; y < S; y += 2)
+                    *reinterpret_cast<uint16_t *>(d + y) = 0;
+        }
+    }
+}
+
+__global__ void batch_copy_kernel(const uint8_t *const *__restrict__ src,
+                                  uint8_t *const *__restrict__ dst,
+                                  const unsigned long long *__restrict__ bytes, int n)
+{
+    for (int j = blockIdx.y; j < n; j += gridDim.y) {
+        const uint8_t *s = src[j];
+        uint8_t *d = dst[j];
+        const size_t S = bytes[j];
+        for (size_t x = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 16; x < S;
+             x += static_cast<size_t>(gridDim.x) * blockDim.x * 16) {
+            if (x + 16 <= S)
+                *reinterpret_cast<uint4 *>(d + x) = *reinterpret_cast<const uint4 *>(s + x);
+            else
+                for (size_t y = x; y < S; y += 2)
+                    *reinterpret_cast<uint16_t *>(d + y) = *reinterpret_cast<const uint16_t *>(s + y);
+        }
+    }
+}
+
+static unsigned grid_for(unsigned long long n)
+{
+    return static_cast<unsigned>((n + 255) / 256);
+}
+
+int batch_planes(cudaStream_t st, const PlanesProb *d, int np, unsigned long long total)
+{
+    if (!total)
+        return P2G_OK;
+    batch_planes_kernel<<<grid_for(total), 256, 0, st>>>(d, np, total);
+    P2G_CUDA(cudaGetLastError());
+    return P2G_OK;
+}
+
+int batch_records(cudaStream_t st, const uint16_t *glog, const uint16_t *gexp, const RecProb *d,
+                  int np, unsigned long long total)
+{
+    if (!total)
+        return P2G_OK;
+    batch_records_kernel<<<grid_for(total), 256, 0, st>>>(d, np, total, glog, gexp);
+    P2G_CUDA(cudaGetLastError());
+    return P2G_OK;
+}
+
+int batch_zero(cudaStream_t st, uint8_t *const *ptrs, const unsigned long long *bytes, int n)
+{
+    if (n <= 0)
+        return P2G_OK;
+    batch_zero_kernel<<<dim3(16, std::min(n, 4096)), 256, 0, st>>>(ptrs, bytes, n);
+    P2G_CUDA(cudaGetLastError());
+    return P2G_OK;
+}
+
+int batch_copy(cudaStream_t st, const uint8_t *const *src, uint8_t *const *dst,
+               const unsigned long long *bytes, int n)
+{
+    if (n <= 0)
+        return P2G_OK;
+    batch_copy_kernel<<<dim3(16, std::min(n, 4096)), 256, 0, st>>>(src, dst, bytes, n);
+    P2G_CUDA(cudaGetLastError());
+    return P2G_OK;
+}
+
+int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchItem *items,
+                 int nitems, int *counter)
+{
+    if (nitems <= 0)
+        return P2G_OK;
+    constexpr int W = kBatchWarps, E = kBatchEreg;
+    MuladdPlan p;
+    p.warps = W;
+    p.ereg = E;
+    const size_t smem = smem_bytes(p);
+    auto fn = muladd_persistent<W, E, 1>;
+    P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    fn<<<grid, W * 32, smem, st>>>(probs, items, nitems, counter);
+    P2G_CUDA(cudaGetLastError());
     return P2G_OK;
 }
 

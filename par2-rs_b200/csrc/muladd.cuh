@@ -4,6 +4,52 @@
 
 namespace p2g {
 
+// One multiply-accumulate problem of a batch (device-resident description).
+struct BatchProb {
+    const uint32_t *planes;  // [nin][T][512]
+    const uint32_t *recs;    // [nin][nout][16]
+    uint8_t *const *dst;     // nout device pointers
+    size_t S;                // bytes per slice
+    int nin, nout, T, nblk, nsplit, mode;
+};
+// One work item of a batch: (problem, column tile, output block, input split).
+struct BatchItem {
+    int prob, t, ob, split;
+};
+// Shape of the persistent batch kernel: 8 warps x 13 outputs (104 per block).
+constexpr int kBatchWarps = 8, kBatchEreg = 13, kBatchBlock = kBatchWarps * kBatchEreg;
+
+// Bit-plane conversion of one problem of a batch; `first` is the problem's
+// first thread in the batched grid (nin * T * 32 threads each).
+struct PlanesProb {
+    const uint8_t *const *src;
+    uint32_t *planes;
+    size_t S;
+    int nin, T;
+    unsigned long long first;
+};
+// Records of one problem: coefficient (i, o) from a [nout][nin] matrix, or
+// consts[i]^exps[o]; nin * nout threads each.
+struct RecProb {
+    const uint16_t *consts;
+    const uint32_t *exps;
+    const uint16_t *coeff;
+    uint32_t *recs;
+    int nin, nout;
+    unsigned long long first;
+};
+
+int batch_planes(cudaStream_t st, const PlanesProb *d, int np, unsigned long long total);
+int batch_records(cudaStream_t st, const uint16_t *glog, const uint16_t *gexp, const RecProb *d,
+                  int np, unsigned long long total);
+int batch_zero(cudaStream_t st, uint8_t *const *ptrs, const unsigned long long *bytes, int n);
+int batch_copy(cudaStream_t st, const uint8_t *const *src, uint8_t *const *dst,
+               const unsigned long long *bytes, int n);
+// The persistent kernel over `nitems` items (longest first) with `grid` CTAs;
+// *counter must be zero.
+int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchItem *items,
+                 int nitems, int *counter);
+
 // The plan for a problem: the context's tuned plan for this shape if there
 // is one, else a heuristic (8 warps, as many outputs per warp as fit).
 MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t slice_bytes);

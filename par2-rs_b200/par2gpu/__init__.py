@@ -56,8 +56,25 @@ SIGNATURES = [
     ("p2g_hash_slices", _I, [_P, _P, _S, _S, _P, _P, _U32]),
     ("p2g_verify_slices", _I, [_P, _P, _S, _S, _P, _P, _P, _U32]),
     ("p2g_encode_noalloc", _I, [_P, _P, _S, _S, _P, _S, _P]),
+    ("p2g_batch_create", _I, [_P, _P, _S, _U32, _P]),
+    ("p2g_batch_run", _I, [_P]),
+    ("p2g_batch_launch", _I, [_P]),
+    ("p2g_batch_poll", _I, [_P, _P]),
+    ("p2g_batch_wait", _I, [_P]),
+    ("p2g_batch_destroy", _I, [_P]),
 ]
+JOB_CREATE, JOB_REPAIR, JOB_VERIFY = 1, 2, 3
+BATCH_GRAPH = 0x2
+
+
+class Job(ctypes.Structure):
+    """p2g_job: one create / repair / verify job of a batch."""
+    _fields_ = [("kind", _I), ("k", _S), ("slice_bytes", _S), ("col_begin", _S),
+                ("col_end", _S), ("src", _P), ("n", _S), ("exps", _P), ("missing", _P),
+                ("recovery", _P), ("inverse", _P), ("out", _P), ("md5_out", _P),
+                ("crc_out", _P), ("status", _I)]
 NOALLOC_SCRATCH_BYTES = 64 << 20
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: the legacy default stream
 
 
 class Timing(ctypes.Structure):
@@ -132,7 +149,8 @@ def encode_noalloc(stream, srcs, slice_bytes, exps, outs):
     fixed static scratch only (for callers that cannot allocate); enqueued on
     `stream` (an int cudaStream_t handle, 0 = default stream), not waited for."""
     e = np.ascontiguousarray(exps, np.uint32)
-    check(lib().p2g_encode_noalloc(stream or None, _ptr_array(srcs), len(srcs), slice_bytes,
+    check(lib().p2g_encode_noalloc(stream if stream else None, _ptr_array(srcs), len(srcs),
+                                   slice_bytes,
                                    e.ctypes.data, len(e), _ptr_array(outs)))
 
 
@@ -177,9 +195,13 @@ class Context:
             pass
 
     def set_stream(self, stream):
-        """Run on a caller CUDA stream (int handle, e.g. torch's
-        ``cuda_stream``); None restores the context's own stream."""
-        check(lib().p2g_set_stream(self.h, stream or None))
+        """Run on a caller CUDA stream: an int cudaStream_t handle such as
+        torch's ``cuda_stream`` (0, the legacy default stream, is passed as
+        cudaStreamLegacy); None restores the context's own stream."""
+        if stream is None:
+            check(lib().p2g_set_stream(self.h, None))
+        else:
+            check(lib().p2g_set_stream(self.h, stream if stream else CUDA_STREAM_LEGACY))
 
     def set_timing(self, enable=True):
         check(lib().p2g_set_timing(self.h, 1 if enable else 0))
@@ -290,3 +312,88 @@ class Context:
                                       md5e.ctypes.data, crce.ctypes.data, ok.ctypes.data,
                                       DEVICE_PTRS if device else 0))
         return ok.astype(bool)
+
+
+class Batch:
+    """A batch of jobs (p2g_batch_*).  Each job is a dict:
+      create: kind=JOB_CREATE, k, slice_bytes, src (k device ptrs), exps, out (r ptrs)
+      repair: kind=JOB_REPAIR, k, slice_bytes, src (k-m present ptrs), missing, exps,
+              recovery (m ptrs), out (m ptrs), optional inverse (m x m uint16)
+      verify: kind=JOB_VERIFY, k, slice_bytes, src (k ptrs) -> result md5 [k,16], crc [k]
+    optional col_begin / col_end restrict create / repair to a byte range.
+    Pointers are ints or torch CUDA tensors."""
+
+    def __init__(self, ctx, jobs, graph=False):
+        self.ctx = ctx
+        self._keep = []
+        self.jobs = (Job * max(1, len(jobs)))()
+        self.specs = jobs
+        self.results = []
+        for j, spec in enumerate(jobs):
+            J = self.jobs[j]
+            J.kind = spec["kind"]
+            J.k = spec["k"]
+            J.slice_bytes = spec["slice_bytes"]
+            J.col_begin = spec.get("col_begin", 0)
+            J.col_end = spec.get("col_end", 0)
+            src = _ptr_array(spec["src"])
+            self._keep.append(src)
+            J.src = ctypes.cast(src, ctypes.c_void_p)
+            res = {}
+            if spec["kind"] in (JOB_CREATE, JOB_REPAIR):
+                e = np.ascontiguousarray(spec["exps"], np.uint32)
+                out = _ptr_array(spec["out"])
+                self._keep += [e, out]
+                J.n = len(e)
+                J.exps = e.ctypes.data
+                J.out = ctypes.cast(out, ctypes.c_void_p)
+            if spec["kind"] == JOB_REPAIR:
+                miss = np.ascontiguousarray(spec["missing"], np.uint64)
+                rec = _ptr_array(spec["recovery"])
+                self._keep += [miss, rec]
+                J.missing = miss.ctypes.data
+                J.recovery = ctypes.cast(rec, ctypes.c_void_p)
+                if spec.get("inverse") is not None:
+                    inv = np.ascontiguousarray(spec["inverse"], np.uint16)
+                    self._keep.append(inv)
+                    J.inverse = inv.ctypes.data
+            if spec["kind"] == JOB_VERIFY:
+                res["md5"] = np.zeros((spec["k"], 16), np.uint8)
+                res["crc"] = np.zeros(spec["k"], np.uint32)
+                J.md5_out = res["md5"].ctypes.data
+                J.crc_out = res["crc"].ctypes.data
+            self.results.append(res)
+        h = ctypes.c_void_p()
+        check(lib().p2g_batch_create(ctx.h, ctypes.cast(self.jobs, ctypes.c_void_p), len(jobs),
+                                     BATCH_GRAPH if graph else 0, ctypes.byref(h)))
+        self.h = h
+
+    def run(self):
+        check(lib().p2g_batch_run(self.h))
+        return [self.jobs[j].status for j in range(len(self.specs))]
+
+    def launch(self):
+        check(lib().p2g_batch_launch(self.h))
+
+    def poll(self):
+        d = ctypes.c_int()
+        check(lib().p2g_batch_poll(self.h, ctypes.byref(d)))
+        return bool(d.value)
+
+    def wait(self):
+        check(lib().p2g_batch_wait(self.h))
+        return [self.jobs[j].status for j in range(len(self.specs))]
+
+    def statuses(self):
+        return [self.jobs[j].status for j in range(len(self.specs))]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().p2g_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -171,3 +171,20 @@ def test_set_plan_rejects_uncompiled_shapes(ctx):
     with pytest.raises(par2gpu.Par2GpuError) as ei:
         ctx.set_plan(10, 20, 4096, 16, 9, 1, 1)
     assert ei.value.code == par2gpu.EINVAL
+
+
+def test_caller_default_stream_is_ordered(ctx):
+    """Work on torch's default stream (handle 0) must be ordered with the
+    context's work once the context runs on that stream."""
+    import torch
+
+    k, S, r = 64, 65536, 5
+    src = torch.randint(0, 256, (k, S), dtype=torch.uint8, device="cuda")  # queued, not waited
+    out = torch.zeros((r, S), dtype=torch.uint8, device="cuda")
+    exps = np.arange(r, dtype=np.uint32)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    try:
+        ctx.encode([src[i] for i in range(k)], S, exps, [out[e] for e in range(r)], device=True)
+    finally:
+        ctx.set_stream(None)
+    assert np.array_equal(out.cpu().numpy(), oracle.encode(src.cpu().numpy(), exps))
