@@ -589,6 +589,94 @@ def run_batched(args):
     print(json.dumps(out), flush=True)
 
 
+def serving_pool(dev, nsets, seed):
+    """Device-resident job data for the serving loop: sets drawn from the
+    batched distribution; each arrival becomes a create (40 %), verify (40 %)
+    or repair (20 %) job over one of them."""
+    import torch
+
+    sets = batched_sets(seed, nsets)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 1)
+    pool = []
+    for x in sets:
+        src = torch.randint(0, 256, (x["k"], x["S"]), dtype=torch.uint8, device=dev, generator=g)
+        pool.append({"spec": x, "src": src})
+    return pool
+
+
+def make_jobs(pool, nj, rng, ctx):
+    import torch
+
+    from par2gpu.serve import ServedJob
+
+    jobs = []
+    for jid in range(nj):
+        p = pool[int(rng.integers(len(pool)))]
+        x = p["spec"]
+        u = rng.uniform()
+        if u < 0.4:
+            jobs.append(ServedJob(jid, "create", p["src"], r=x["r"]))
+        elif u < 0.8:
+            jobs.append(ServedJob(jid, "verify", p["src"]))
+        else:
+            if "rec" not in p:
+                m = max(1, min(x["k"], x.get("m", 1)))
+                # own generator: both job lists must draw the same sequence
+                prng = np.random.default_rng(x["k"] * 7919 + x["S"])
+                miss = np.sort(prng.choice(x["k"], m, replace=False))
+                rec = torch.zeros((m, x["S"]), dtype=torch.uint8, device=p["src"].device)
+                ctx.encode([p["src"][i] for i in range(x["k"])], x["S"], np.arange(m),
+                           [rec[q] for q in range(m)], device=True)
+                p["rec"], p["miss"] = rec, miss
+            jobs.append(ServedJob(jid, "repair", p["src"], missing=p["miss"], rec=p["rec"]))
+    return jobs
+
+
+def run_serving(args):
+    """Poisson arrivals at rates 10..2000 jobs/s; continuous batching versus
+    one job at a time on the same GPU and the same arrival times; jobs/s and
+    p50/p95/p99 latency; every job's outputs compared between the two."""
+    import torch
+
+    import par2gpu
+    from par2gpu.serve import latency_stats, serve_continuous, serve_one_at_a_time
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ctxs = [par2gpu.Context(0), par2gpu.Context(0), par2gpu.Context(0)]
+    pool = serving_pool(dev, 48, SEED + 21)
+    torch.cuda.synchronize(dev)
+    results = []
+    for lam in (10, 100, 500, 1000, 2000):
+        rng = np.random.default_rng(SEED + lam)
+        nj = int(min(240, max(40, lam * 1.5)))
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, nj))
+        jobs_a = make_jobs(pool, nj, np.random.default_rng(SEED + 100 + lam), ctxs[0])
+        jobs_b = make_jobs(pool, nj, np.random.default_rng(SEED + 100 + lam), ctxs[0])
+        torch.cuda.synchronize(dev)
+        lat_a, wall_a = serve_continuous(ctxs, jobs_a, arrivals)
+        torch.cuda.synchronize(dev)
+        lat_b, wall_b = serve_one_at_a_time(ctxs[0], jobs_b, arrivals)
+        torch.cuda.synchronize(dev)
+        same = True
+        for ja, jb in zip(jobs_a, jobs_b):
+            if ja.kind == "verify":
+                same = same and np.array_equal(ja.md5, jb.md5) and np.array_equal(ja.crc, jb.crc)
+            else:
+                same = same and bool(torch.equal(ja.out, jb.out))
+        results.append({"rate_jobs_per_s": lam, "continuous": latency_stats(lat_a, wall_a),
+                        "one_at_a_time": latency_stats(lat_b, wall_b),
+                        "outputs_identical": bool(same)})
+        del jobs_a, jobs_b
+    for c in ctxs:
+        c.close()
+    print(json.dumps({"workload": "serving: Poisson arrivals, 40% create / 40% verify / "
+                                  "20% repair, sizes from the batched distribution (48 "
+                                  "device-resident sets), 120 GB admission budget",
+                      "sweep": results}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -596,7 +684,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large_encode",
-                    choices=sorted(WORKLOADS) + ["verify_repair", "batched"])
+                    choices=sorted(WORKLOADS) + ["verify_repair", "batched", "serving"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the heuristic tile shape instead of the autotuned one")
     ap.add_argument("--quick", action="store_true",
@@ -607,6 +695,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args)
+        return
+    if args.workload == "serving":
+        run_serving(args)
         return
     global K_SRC, SLICE, R_REC, WORKLOAD
     K_SRC, SLICE, R_REC, WORKLOAD = WORKLOADS[args.workload]

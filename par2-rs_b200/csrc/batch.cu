@@ -579,11 +579,16 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
             set_error("p2g_batch_create: %s", cudaGetErrorString(cudaGetLastError()));
             return fail(P2G_ECUDA);
         }
+        // capture on the context's own stream (the caller's may be the legacy
+        // default stream, which cannot be captured); replays go to ctx->stream
         const bool timing = ctx->timing;
+        cudaStream_t caller = ctx->stream;
         ctx->timing = false;  // no event records inside the graph
+        ctx->stream = ctx->own_stream;
         cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
         int rc = e == cudaSuccess ? enqueue(b) : P2G_ECUDA;
         cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &b->graph);
+        ctx->stream = caller;
         ctx->timing = timing;
         if (rc != P2G_OK || e2 != cudaSuccess ||
             cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {

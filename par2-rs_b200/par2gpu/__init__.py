@@ -164,8 +164,16 @@ def _ptr(x):
 
 
 def _ptr_array(xs):
+    """A C array of pointers: from a numpy uint64 array of addresses (used as
+    is), or from a list of ints / tensors / arrays."""
+    if isinstance(xs, np.ndarray) and xs.dtype == np.uint64:
+        return np.ascontiguousarray(xs) if len(xs) else np.zeros(1, np.uint64)
     arr = (ctypes.c_void_p * max(1, len(xs)))(*[_ptr(x) for x in xs])
     return arr
+
+
+def _as_voidp(a):
+    return a.ctypes.data if isinstance(a, np.ndarray) else ctypes.cast(a, ctypes.c_void_p)
 
 
 class Context:
@@ -338,7 +346,7 @@ class Batch:
             J.col_end = spec.get("col_end", 0)
             src = _ptr_array(spec["src"])
             self._keep.append(src)
-            J.src = ctypes.cast(src, ctypes.c_void_p)
+            J.src = _as_voidp(src)
             res = {}
             if spec["kind"] in (JOB_CREATE, JOB_REPAIR):
                 e = np.ascontiguousarray(spec["exps"], np.uint32)
@@ -346,13 +354,13 @@ class Batch:
                 self._keep += [e, out]
                 J.n = len(e)
                 J.exps = e.ctypes.data
-                J.out = ctypes.cast(out, ctypes.c_void_p)
+                J.out = _as_voidp(out)
             if spec["kind"] == JOB_REPAIR:
                 miss = np.ascontiguousarray(spec["missing"], np.uint64)
                 rec = _ptr_array(spec["recovery"])
                 self._keep += [miss, rec]
                 J.missing = miss.ctypes.data
-                J.recovery = ctypes.cast(rec, ctypes.c_void_p)
+                J.recovery = _as_voidp(rec)
                 if spec.get("inverse") is not None:
                     inv = np.ascontiguousarray(spec["inverse"], np.uint16)
                     self._keep.append(inv)
