@@ -67,16 +67,84 @@ struct p2g_batch {
     size_t copy_src_off = 0, copy_dst_off = 0, copy_len_off = 0, counter_off = 0;
     int ncopy = 0;
     std::vector<HashGroup> hash;
+    size_t hash_bytes = 0;  // MD5 + CRC results of all groups
     DevBuf hash_host;  // pinned
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done = nullptr;
     bool launched = false;
+    bool recorded = false;  // `done` has been recorded at least once
 };
 
 namespace {
 
 uint8_t *dp(p2g_batch *b, size_t off) { return b->params.as<uint8_t>() + off; }
+
+constexpr size_t kMaxSpare = 32;
+
+// Gives `d` (empty on entry) at least `need` bytes: the smallest spare buffer
+// of the context that fits, else a new allocation with 25 % headroom so that
+// batches of similar size reuse it.  ctx->mu must be held.
+int take(p2g_ctx *ctx, DevBuf &d, size_t need)
+{
+    if (need <= d.cap)
+        return P2G_OK;
+    size_t best = ctx->spare.size();
+    for (size_t i = 0; i < ctx->spare.size(); ++i) {
+        const DevBuf &x = ctx->spare[i];
+        if (x.pinned == d.pinned && x.cap >= need &&
+            (best == ctx->spare.size() || x.cap < ctx->spare[best].cap))
+            best = i;
+    }
+    if (best < ctx->spare.size()) {
+        d.release();
+        d = ctx->spare[best];
+        ctx->spare.erase(ctx->spare.begin() + static_cast<long>(best));
+        return P2G_OK;
+    }
+    return d.ensure(need + need / 4);
+}
+
+// Returns `d` to the context's spares (the GPU no longer uses it); beyond
+// kMaxSpare buffers the smallest ones are freed.  ctx->mu must be held.
+void give(p2g_ctx *ctx, DevBuf &d)
+{
+    if (d.p)
+        ctx->spare.push_back(d);
+    d = DevBuf{};
+    while (ctx->spare.size() > kMaxSpare) {
+        size_t small = 0;
+        for (size_t i = 1; i < ctx->spare.size(); ++i)
+            if (ctx->spare[i].cap < ctx->spare[small].cap)
+                small = i;
+        ctx->spare[small].release();
+        ctx->spare.erase(ctx->spare.begin() + static_cast<long>(small));
+    }
+}
+
+// Frees a batch.  Its buffers go back to the context only once every
+// operation that touches them has completed (b->done is recorded after the
+// create-time uploads and again after each launch).  ctx->mu must be held.
+void batch_free(p2g_batch *b)
+{
+    if (b->done && b->recorded)
+        cudaEventSynchronize(b->done);
+    if (b->exec)
+        cudaGraphExecDestroy(b->exec);
+    if (b->graph)
+        cudaGraphDestroy(b->graph);
+    if (b->done)
+        cudaEventDestroy(b->done);
+    DevBuf *bufs[] = {&b->params, &b->hparams, &b->planes, &b->recs, &b->rhs,
+                      &b->inv,    &b->hashbuf, &b->hash_host};
+    for (DevBuf *d : bufs) {
+        if (b->ctx)
+            give(b->ctx, *d);
+        else
+            d->release();
+    }
+    delete b;
+}
 
 int enqueue(p2g_batch *b)
 {
@@ -189,8 +257,18 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
     b->njobs = njobs;
     b->hparams.pinned = true;
     b->hash_host.pinned = true;
+    if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) {
+        (void)cudaGetLastError();
+        delete b;
+        set_error("p2g_batch_create: cudaEventCreate failed");
+        return P2G_ECUDA;
+    }
+    // on failure, wait for the uploads already queued before reusing buffers
     auto fail = [&](int rc) {
-        p2g_batch_destroy(b);
+        if (cudaEventRecord(b->done, ctx->stream) == cudaSuccess)
+            b->recorded = true;
+        (void)cudaGetLastError();
+        batch_free(b);
         return rc;
     };
     // ---- decode matrices of REPAIR jobs ----
@@ -201,13 +279,13 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
             inv_off[j] = inv_bytes;
             inv_bytes += al256(jobs[j].n * jobs[j].n * 2);
         }
-    if (int rc = b->inv.ensure(inv_bytes + 256))
+    if (int rc = take(ctx, b->inv, inv_bytes + 256))
         return fail(rc);
     std::vector<int> singular(njobs, 0);
     {
         std::vector<int> pending;
         DevBuf stat;
-        if (int rc = stat.ensure(njobs * sizeof(int) + 16))
+        if (int rc = take(ctx, stat, njobs * sizeof(int) + 16))
             return fail(rc);
         std::vector<uint8_t> h;
         for (size_t j = 0; j < njobs; ++j) {
@@ -219,7 +297,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
                 if (cudaMemcpyAsync(d_inv, J.inverse, J.n * J.n * 2, cudaMemcpyHostToDevice,
                                     ctx->stream) != cudaSuccess) {
                     set_error("p2g_batch_create: decode matrix upload failed");
-                    stat.release();
+                    give(ctx, stat);
                     return fail(P2G_ECUDA);
                 }
                 continue;
@@ -250,7 +328,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
             // the pageable host source is consumed before the next iteration
             // reuses `h`, and ctx->coeffs before the next upload (stream order)
             if (rc != P2G_OK) {
-                stat.release();
+                give(ctx, stat);
                 return fail(rc);
             }
             pending.push_back(static_cast<int>(j));
@@ -262,7 +340,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
                 cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
                 set_error("p2g_batch_create: inversion failed: %s",
                           cudaGetErrorString(cudaGetLastError()));
-                stat.release();
+                give(ctx, stat);
                 return fail(P2G_ECUDA);
             }
             for (int j : pending)
@@ -271,7 +349,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
                     jobs[j].status = P2G_ESINGULAR;
                 }
         }
-        stat.release();
+        give(ctx, stat);
     }
     // ---- problems ----
     Image img;
@@ -286,7 +364,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
             rhs_off[j] = rhs_bytes;
             rhs_bytes += al256(jobs[j].n * al16(S));
         }
-    if (int rc = b->rhs.ensure(rhs_bytes + 256))
+    if (int rc = take(ctx, b->rhs, rhs_bytes + 256))
         return fail(rc);
     std::vector<HashGroup> hg;
     for (size_t j = 0; j < njobs; ++j) {
@@ -396,9 +474,9 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
         plane_need = std::max(plane_need, pl);
         rec_need = std::max(rec_need, rc);
     }
-    if (int rc = b->planes.ensure(plane_need + 256))
+    if (int rc = take(ctx, b->planes, plane_need + 256))
         return fail(rc);
-    if (int rc = b->recs.ensure(rec_need + 256))
+    if (int rc = take(ctx, b->recs, rec_need + 256))
         return fail(rc);
     b->copy_src_off = img.put(copy_src.data(), copy_src.size() * sizeof(void *));
     b->copy_dst_off = img.put(copy_dst.data(), copy_dst.size() * sizeof(void *));
@@ -533,7 +611,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
             ptrs[i] = jobs[g.slices[i].first].src[g.slices[i].second];
         g.ptr_off = img.put(ptrs.data(), ptrs.size() * sizeof(void *));
     }
-    if (int rc = b->params.ensure(img.bytes.size() + 256))
+    if (int rc = take(ctx, b->params, img.bytes.size() + 256))
         return fail(rc);
     uint8_t *base = b->params.as<uint8_t>();
     auto rebase = [&](const void *off) { return base + reinterpret_cast<uintptr_t>(off); };
@@ -559,21 +637,23 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
         g.out_off = hbytes;
         hbytes += al256(al16(static_cast<size_t>(g.n) * 16) + static_cast<size_t>(g.n) * 4);
     }
-    if (int rc = b->hashbuf.ensure(hbytes + 256))
+    if (int rc = take(ctx, b->hashbuf, hbytes + 256))
         return fail(rc);
     if (hbytes)
-        if (int rc = b->hash_host.ensure(hbytes + 256))
+        if (int rc = take(ctx, b->hash_host, hbytes + 256))
             return fail(rc);
     b->hash = hg;
-    if (int rc = b->hparams.ensure(img.bytes.size() + 256))
+    b->hash_bytes = hbytes;
+    if (int rc = take(ctx, b->hparams, img.bytes.size() + 256))
         return fail(rc);
     memcpy(b->hparams.p, img.bytes.data(), img.bytes.size());
     if (cudaMemcpyAsync(b->params.p, b->hparams.p, img.bytes.size(), cudaMemcpyHostToDevice,
                         ctx->stream) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventRecord(b->done, ctx->stream) != cudaSuccess) {
         set_error("p2g_batch_create: table upload failed");
         return fail(P2G_ECUDA);
     }
+    b->recorded = true;
     if (flags & P2G_BATCH_GRAPH) {
         if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
             set_error("p2g_batch_create: %s", cudaGetErrorString(cudaGetLastError()));
@@ -621,8 +701,8 @@ int p2g_batch_launch(p2g_batch *b)
     } else {
         P2G_TRY(enqueue(b));
     }
-    if (b->hash_host.p)
-        P2G_CUDA(cudaMemcpyAsync(b->hash_host.p, b->hashbuf.p, b->hash_host.cap,
+    if (b->hash_bytes)
+        P2G_CUDA(cudaMemcpyAsync(b->hash_host.p, b->hashbuf.p, b->hash_bytes,
                                  cudaMemcpyDeviceToHost, ctx->stream));
     ctx->mark(4);
     P2G_CUDA(cudaEventRecord(b->done, ctx->stream));
@@ -698,26 +778,16 @@ int p2g_batch_destroy(p2g_batch *b)
 {
     if (!b)
         return P2G_OK;
-    if (b->ctx) {
-        cudaSetDevice(b->ctx->device);
-        if (b->launched && b->done)
-            cudaEventSynchronize(b->done);
+    if (!b->ctx) {
+        batch_free(b);
+        return P2G_OK;
     }
-    if (b->exec)
-        cudaGraphExecDestroy(b->exec);
-    if (b->graph)
-        cudaGraphDestroy(b->graph);
-    if (b->done)
-        cudaEventDestroy(b->done);
-    b->params.release();
-    b->hparams.release();
-    b->planes.release();
-    b->recs.release();
-    b->rhs.release();
-    b->inv.release();
-    b->hashbuf.release();
-    b->hash_host.release();
-    delete b;
+    cudaSetDevice(b->ctx->device);
+    // wait outside the lock: other batches of the context may be created meanwhile
+    if (b->done && b->recorded)
+        cudaEventSynchronize(b->done);
+    std::lock_guard<std::mutex> lock(b->ctx->mu);
+    batch_free(b);
     return P2G_OK;
 }
 

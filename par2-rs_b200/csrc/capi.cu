@@ -357,6 +357,9 @@ int p2g_destroy(p2g_ctx *ctx)
     if (ctx->d_crc)
         cudaFree(ctx->d_crc);
     ctx->hash_out.release();
+    for (p2g::DevBuf &d : ctx->spare)
+        d.release();
+    ctx->spare.clear();
     for (cudaEvent_t e : ctx->ev)
         if (e)
             cudaEventDestroy(e);

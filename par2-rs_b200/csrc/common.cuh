@@ -8,6 +8,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "../../include/par2gpu.h"
 
@@ -94,6 +95,10 @@ struct p2g_ctx {
     p2g::DevBuf gj_M;      // Gauss-Jordan augmented matrix
     p2g::DevBuf gj_status; // Gauss-Jordan status + pivots
     p2g::DevBuf hash_out;  // MD5 + CRC results
+    // Scratch buffers of destroyed batches, kept for the next batch: freeing
+    // device or pinned memory synchronises the whole device, which would stall
+    // a batch being prepared while another one runs.  Guarded by `mu`.
+    std::vector<p2g::DevBuf> spare;
 };
 
 #define P2G_CUDA(call)                                                                  \

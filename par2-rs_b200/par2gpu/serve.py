@@ -148,7 +148,9 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
         return time.perf_counter() - t0
 
     def build(ctx):
-        """Pick units round-robin from admitted jobs up to the iteration budget."""
+        """Pick units round-robin from admitted jobs up to the iteration
+        budget, then merge each job's contiguous units into one spec so that
+        its coefficient records are built once per batch."""
         picked, work = [], 0.0
         progress = True
         while progress and work < iter_macs:
@@ -167,8 +169,16 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
                     break
         if not picked:
             return None
-        b = Batch(ctx, [_job_spec(j, u) for j, u in picked])
-        return (b, picked)
+        merged = []  # [job, (kind, a, b), units merged]
+        for job, u in sorted(picked, key=lambda p: (p[0].jid, p[1][1])):
+            if merged and merged[-1][0] is job and merged[-1][1][2] == u[1]:
+                last = merged[-1]
+                last[1] = (u[0], last[1][1], u[2])
+                last[2] += 1
+            else:
+                merged.append([job, u, 1])
+        b = Batch(ctx, [_job_spec(j, u) for j, u, _ in merged])
+        return (b, merged)
 
     while done < n:
         t = now()
@@ -189,14 +199,14 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
             b, picked = inflight[0], inflight[1]
             b.wait()
             t = now()
-            for pos, (job, u) in enumerate(picked):
+            for pos, (job, u, cnt) in enumerate(picked):
                 if job.kind == "verify":
                     res = b.results[pos]
                     a, c = u[1], u[2]
                     job.md5[a:c] = res["md5"]
                     job.crc[a:c] = res["crc"]
                 ent = state[job.jid]
-                ent[2] -= 1
+                ent[2] -= cnt
                 if ent[2] == 0:
                     lat[job.jid] = t - arrivals[job.jid]
                     done += 1
