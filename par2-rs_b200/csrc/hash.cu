@@ -11,9 +11,18 @@
 //     final XOR 0xFFFFFFFF, computed four bytes at a time with four 256-entry
 //     tables ("slicing by 4").
 //
-// One thread owns one slice (MD5 is a serial chain over the slice).  The four
-// CRC tables are replicated 32 times in shared memory so that lane L always
-// reads bank L: data-dependent table reads never conflict.
+// One lane owns one slice (MD5 is a serial chain over the slice) and computes
+// both checksums from the same registers.  The 32 slices of a warp stream
+// through a 3-stage shared-memory ring filled by cp.async: eight lanes copy
+// 128 contiguous bytes of one slice (coalesced), the 16-byte units of each
+// slice row are XOR-swizzled by the slice index so that the lanes' 16-byte
+// reads of their own rows never conflict, and the copy of chunk c+2 is in
+// flight while chunk c is hashed.  The four CRC tables are replicated 32 times
+// in shared memory so that lane L always reads bank L: data-dependent table
+// reads never conflict.
+#include <algorithm>
+
+#include "async.cuh"
 #include "hash.cuh"
 
 namespace p2g {
@@ -77,69 +86,166 @@ __device__ __forceinline__ void md5_block(uint32_t st[4], const uint32_t x[16])
 }
 
 constexpr int kHashThreads = 256;
+constexpr int kHashWarps = kHashThreads / 32;
 constexpr int kCrcTabWords = 4 * 256 * 32;  // 4 tables x 256 entries x 32 bank copies
+constexpr int kChunk = 128;                 // bytes of every slice per ring stage
+constexpr int kStages = 3;
+constexpr int kStageBytes = 32 * kChunk;    // one warp's 32 slices
+constexpr size_t kHashSmem =
+    static_cast<size_t>(kCrcTabWords) * 4 + static_cast<size_t>(kHashWarps) * kStages * kStageBytes;
 
-// table t, entry e, for this lane
-__device__ __forceinline__ uint32_t crc_tab(const uint32_t *stab, int t, uint32_t e, int lane)
+// CRC table layout in shared memory: tables 2p and 2p+1 share a 64 KiB
+// region p, whose row e (256 bytes) holds entry e of table 2p in its first
+// 128 bytes and of table 2p+1 in its second, 32 copies each -- copy L for
+// lane L, so every lane reads its own bank.  The byte offset of (table T,
+// entry e, lane L) is then base_T(L) with e placed in its byte 1, one PRMT.
+__device__ __forceinline__ uint32_t crc_base(int T, int lane)
 {
-    return stab[((t << 8) + e) * 32 + lane];
+    return static_cast<uint32_t>((T >> 1) << 16 | (T & 1) << 7 | lane << 2);
+}
+__device__ __forceinline__ uint32_t crc_at(const uint32_t *stab, uint32_t off)
+{
+    return *reinterpret_cast<const uint32_t *>(reinterpret_cast<const uint8_t *>(stab) + off);
 }
 
-__device__ __forceinline__ uint32_t crc_word(const uint32_t *stab, uint32_t crc, uint32_t w, int lane)
+struct CrcLanes {
+    uint32_t b0, b1, b2, b3;  // crc_base(T, lane) for T = 0..3
+};
+
+// slicing by 4: crc' = T3[t.b0] ^ T2[t.b1] ^ T1[t.b2] ^ T0[t.b3], t = crc ^ w
+__device__ __forceinline__ uint32_t crc_word(const uint32_t *stab, uint32_t crc, uint32_t w,
+                                             const CrcLanes &L)
 {
-    crc ^= w;
-    return crc_tab(stab, 3, crc & 0xFF, lane) ^ crc_tab(stab, 2, (crc >> 8) & 0xFF, lane) ^
-           crc_tab(stab, 1, (crc >> 16) & 0xFF, lane) ^ crc_tab(stab, 0, crc >> 24, lane);
+    const uint32_t t = crc ^ w;
+    return crc_at(stab, __byte_perm(t, L.b3, 0x7604)) ^ crc_at(stab, __byte_perm(t, L.b2, 0x7614)) ^
+           crc_at(stab, __byte_perm(t, L.b1, 0x7624)) ^ crc_at(stab, __byte_perm(t, L.b0, 0x7634));
 }
 
-__device__ __forceinline__ uint32_t crc_byte(const uint32_t *stab, uint32_t crc, uint32_t b, int lane)
+__device__ __forceinline__ uint32_t crc_byte(const uint32_t *stab, uint32_t crc, uint32_t b,
+                                             const CrcLanes &L)
 {
-    return crc_tab(stab, 0, (crc ^ b) & 0xFF, lane) ^ (crc >> 8);
+    return crc_at(stab, __byte_perm(crc ^ b, L.b0, 0x7604)) ^ (crc >> 8);
+}
+
+// byte offset of 16-byte unit u of slice row s inside a stage
+__device__ __forceinline__ int stage_pos(int s, int u) { return s * kChunk + ((u ^ (s & 7)) << 4); }
+
+// Copies bytes [off, off + kChunk) of the warp's slices into a stage: lane L
+// moves unit L % 8 of slices L / 8, 4 + L / 8, ... (null pointer: no slice).
+__device__ __forceinline__ void stage_chunk(uint8_t *stage, const uint8_t *const ptr[8], size_t off,
+                                            int lane)
+{
+    const int u = lane & 7;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int s = 4 * i + (lane >> 3);
+        if (ptr[i])
+            cp_async16(stage + stage_pos(s, u), ptr[i] + off + u * 16);
+    }
+}
+
+__device__ __forceinline__ void hash_block(const uint32_t *stab, uint32_t st[4], uint32_t &crc,
+                                           const uint32_t x[16], const CrcLanes &L)
+{
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        crc = crc_word(stab, crc, x[j], L);
+    md5_block(st, x);
 }
 
 __global__ void __launch_bounds__(kHashThreads, 1)
-    hash_slices_kernel(const uint8_t *const *__restrict__ slices, int n, size_t S,
+    hash_slices_kernel(const uint8_t *const *__restrict__ slices, int n, int per_cta, size_t S,
                        const uint32_t *__restrict__ crc_tables, uint8_t *__restrict__ md5_out,
                        uint32_t *__restrict__ crc_out)
 {
-    extern __shared__ uint32_t stab[];
-    for (int idx = threadIdx.x; idx < kCrcTabWords; idx += blockDim.x)
-        stab[idx] = crc_tables[idx >> 5];
+    extern __shared__ __align__(16) uint32_t stab[];
+    for (int idx = threadIdx.x; idx < kCrcTabWords; idx += blockDim.x) {
+        const int L = idx & 31, e = (idx >> 5) & 255, T = idx >> 13;
+        stab[(crc_base(T, L) | e << 8) >> 2] = crc_tables[T * 256 + e];
+    }
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
     const int lane = threadIdx.x & 31;
-    const uint8_t *p = slices[i];
+    const int warp = threadIdx.x >> 5;
+    // this CTA hashes slices [blockIdx * per_cta, end), 32 to a warp
+    const int first = blockIdx.x * per_cta + warp * 32;
+    const int end = min(n, (blockIdx.x + 1) * per_cta);
+    if (first >= end)
+        return;
+    const CrcLanes CL{crc_base(0, lane), crc_base(1, lane), crc_base(2, lane), crc_base(3, lane)};
+    uint8_t *ring = reinterpret_cast<uint8_t *>(stab + kCrcTabWords) +
+                    static_cast<size_t>(warp) * kStages * kStageBytes;
+    const uint8_t *ptr[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int g = first + 4 * i + (lane >> 3);
+        ptr[i] = g < end ? slices[g] : nullptr;
+    }
+    const int me = first + lane;
+    const bool active = me < end;
     uint32_t st[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
     uint32_t crc = 0xFFFFFFFFu;
-    const size_t full = S / 64;
-    const uint4 *q = reinterpret_cast<const uint4 *>(p);
-    for (size_t blk = 0; blk < full; ++blk) {
-        uint32_t x[16];
+    const size_t nch = S / kChunk;
+#pragma unroll
+    for (int c = 0; c < kStages - 1; ++c) {
+        if (static_cast<size_t>(c) < nch)
+            stage_chunk(ring + c * kStageBytes, ptr, static_cast<size_t>(c) * kChunk, lane);
+        cp_async_commit();
+    }
+    int cur = 0;
+    for (size_t c = 0; c < nch; ++c) {
+        cp_async_wait<kStages - 2>();  // this lane's copies of chunk c have landed
+        __syncwarp();                  // ... and every other lane's; chunk c-1 is consumed
+        const size_t pre = c + kStages - 1;
+        const int pst = cur == 0 ? kStages - 1 : cur - 1;
+        if (pre < nch)
+            stage_chunk(ring + pst * kStageBytes, ptr, pre * kChunk, lane);
+        cp_async_commit();
+        if (active) {
+            const uint8_t *row = ring + cur * kStageBytes;
+#pragma unroll
+            for (int b = 0; b < kChunk / 64; ++b) {
+                uint32_t x[16];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const uint4 q = *reinterpret_cast<const uint4 *>(row + stage_pos(lane, 4 * b + v));
+                    x[4 * v] = q.x;
+                    x[4 * v + 1] = q.y;
+                    x[4 * v + 2] = q.z;
+                    x[4 * v + 3] = q.w;
+                }
+                hash_block(stab, st, crc, x, CL);
+            }
+        }
+        cur = cur == kStages - 1 ? 0 : cur + 1;
+    }
+    cp_async_wait<0>();
+    if (!active)
+        return;
+    // the last S % 128 bytes: one more full 64-byte block if there is one,
+    // then the remaining bytes, 0x80, zeros, 64-bit bit length (RFC 1321 3.1-3.2)
+    const uint8_t *t = slices[me] + nch * kChunk;
+    size_t rem = S - nch * kChunk;
+    uint32_t x[16];
+    if (rem >= 64) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(t);
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            uint4 u = __ldg(q + blk * 4 + v);
+            const uint4 u = __ldg(q + v);
             x[4 * v] = u.x;
             x[4 * v + 1] = u.y;
             x[4 * v + 2] = u.z;
             x[4 * v + 3] = u.w;
         }
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
-            crc = crc_word(stab, crc, x[j], lane);
-        md5_block(st, x);
+        hash_block(stab, st, crc, x, CL);
+        t += 64;
+        rem -= 64;
     }
-    // tail: remaining bytes, 0x80, zeros, 64-bit bit length (RFC 1321 3.1-3.2)
-    const size_t rem = S - full * 64;
-    const uint8_t *t = p + full * 64;
-    uint32_t x[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j)
         x[j] = 0;
     for (size_t b = 0; b < rem; ++b) {
         uint32_t v = t[b];
-        crc = crc_byte(stab, crc, v, lane);
+        crc = crc_byte(stab, crc, v, CL);
         x[b >> 2] |= v << (8 * (b & 3));
     }
     x[rem >> 2] |= 0x80u << (8 * (rem & 3));
@@ -153,9 +259,9 @@ __global__ void __launch_bounds__(kHashThreads, 1)
     x[14] = static_cast<uint32_t>(bits);
     x[15] = static_cast<uint32_t>(bits >> 32);
     md5_block(st, x);
-    uint4 *o = reinterpret_cast<uint4 *>(md5_out + static_cast<size_t>(i) * 16);
+    uint4 *o = reinterpret_cast<uint4 *>(md5_out + static_cast<size_t>(me) * 16);
     *o = make_uint4(st[0], st[1], st[2], st[3]);
-    crc_out[i] = crc ^ 0xFFFFFFFFu;
+    crc_out[me] = crc ^ 0xFFFFFFFFu;
 }
 
 void crc32_tables(uint32_t tab[4][256])
@@ -171,7 +277,7 @@ void crc32_tables(uint32_t tab[4][256])
             tab[t][b] = (tab[t - 1][b] >> 8) ^ tab[0][tab[t - 1][b] & 0xFF];
 }
 
-size_t hash_smem_bytes() { return kCrcTabWords * sizeof(uint32_t); }
+size_t hash_smem_bytes() { return kHashSmem; }
 
 int hash_run(p2g_ctx *ctx, const uint8_t *const *d_slices, int n, size_t S, uint8_t *d_md5,
              uint32_t *d_crc)
@@ -181,9 +287,12 @@ int hash_run(p2g_ctx *ctx, const uint8_t *const *d_slices, int n, size_t S, uint
     const size_t smem = hash_smem_bytes();
     P2G_CUDA(cudaFuncSetAttribute(hash_slices_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
-    const int grid = (n + kHashThreads - 1) / kHashThreads;
-    hash_slices_kernel<<<grid, kHashThreads, smem, ctx->stream>>>(d_slices, n, S, ctx->d_crc,
-                                                                  d_md5, d_crc);
+    // spread the slices over every SM (one CTA per SM fits), at most 256 per CTA
+    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    const int per_cta = std::min(kHashThreads, std::max(1, (n + sms - 1) / sms));
+    const int grid = (n + per_cta - 1) / per_cta;
+    hash_slices_kernel<<<grid, kHashThreads, smem, ctx->stream>>>(d_slices, n, per_cta, S,
+                                                                  ctx->d_crc, d_md5, d_crc);
     P2G_CUDA(cudaGetLastError());
     ++ctx->launches;
     return P2G_OK;

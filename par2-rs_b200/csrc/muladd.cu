@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "async.cuh"
 #include "bitslice.cuh"
 #include "muladd.cuh"
 
@@ -38,21 +39,6 @@ constexpr int kTileBytes = 2048;             // 1024 symbols
 constexpr int kTableWords = 512 * 32;        // T0 and T1, 128 B per row
 constexpr int kTableBytes = kTableWords * 4; // 64 KiB
 constexpr int kRing = 4;
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-    uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit()
-{
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 // Four 8x8 b16 matrices from shared memory: lanes 8m..8m+7 give the row
 // addresses of matrix m, lane L receives word L % 4 of row L / 4 of each.

@@ -62,6 +62,18 @@ def test_many_slices_match_oracle(ctx):
     assert np.array_equal(md5, wmd5) and np.array_equal(crc, wcrc)
 
 
+def test_slice_counts_and_chunk_edges(ctx):
+    """Partial warps and CTAs (slices are hashed 32 to a warp, 256 to a CTA)
+    and sizes on both sides of the 128-byte staging chunk and 64-byte block."""
+    rng = np.random.default_rng(9)
+    for n in (1, 31, 33, 257, 600):
+        for S in (64, 127, 128, 129, 191, 192, 193, 255, 256, 384, 1000, 2050):
+            data = rng.integers(0, 256, (n, S), dtype=np.uint8)
+            md5, crc = ctx.hash_slices([data[i] for i in range(n)], S)
+            wmd5, wcrc = oracle.hash_slices(data)
+            assert np.array_equal(md5, wmd5) and np.array_equal(crc, wcrc), (n, S)
+
+
 def test_verify_flags_damage(ctx):
     rng = np.random.default_rng(4)
     data = rng.integers(0, 256, (300, 4096), dtype=np.uint8)
