@@ -367,6 +367,10 @@ def run_verify_repair(args):
                 best = (t.ms_total, t.ms_kernel)
         return best
 
+    if not args.no_autotune:
+        # the encode shape and the two repair passes (present -> RHS, RHS -> missing)
+        out["plans"] = {f"{a}x{b}": ctx.autotune(a, b, S).as_dict()
+                        for a, b in ((k, m), (k - m, m), (m, m))}
     # create: recovery slices of the pristine set
     tot, ker = timed(lambda: ctx.encode(sptr, S, exps, rptr, device=True))
     out["encode"] = {"ms": tot, "kernel_ms": ker, "source_gbs": k * S / tot / 1e6}
@@ -397,7 +401,15 @@ def run_verify_repair(args):
     for _ in range(2):
         ctx.reconstruction_matrix(k, dmg, exps)
         inv_ms.append(ctx.last_timing().ms_total)
-    out["invert"] = {"m": m, "ms": min(inv_ms)}
+    out["invert"] = {"m": m, "ms": min(inv_ms), "method": "closed-form Vandermonde inverse "
+                     "(exponents 0..m-1)"}
+    # the same inversion when the exponents are not consecutive (Gauss-Jordan)
+    gapped = np.concatenate([np.arange(m - 1), [m + 4]]).astype(np.uint32)
+    inv_ms = []
+    for _ in range(2):
+        ctx.reconstruction_matrix(k, dmg, gapped)
+        inv_ms.append(ctx.last_timing().ms_total)
+    out["invert_gapped"] = {"m": m, "ms": min(inv_ms), "method": "blocked Gauss-Jordan"}
     # repair
     fixed = torch.zeros((m, S), dtype=torch.uint8, device=dev)
     fbase = fixed.data_ptr()

@@ -320,7 +320,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
                 rc = gj_invert(ctx, w, static_cast<int>(m), ctx->coeffs.as<uint16_t>(),
                                reinterpret_cast<const uint32_t *>(ctx->coeffs.as<uint8_t>() +
                                                                   al256(m * 2)),
-                               nullptr, d_inv);
+                               J.exps, nullptr, d_inv);
             if (rc == P2G_OK &&
                 cudaMemcpyAsync(stat.as<int>() + j, ctx->gj_status.p, sizeof(int),
                                 cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)

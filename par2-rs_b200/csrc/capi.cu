@@ -643,7 +643,7 @@ int p2g_invert(p2g_ctx *ctx, size_t m, const uint16_t *A, uint16_t *inv)
     P2G_TRY(ctx->inv.ensure(m * m * 2));
     P2G_CUDA(cudaMemcpyAsync(ctx->coeffs.p, A, m * m * 2, cudaMemcpyHostToDevice, ctx->stream));
     GjWork w{ctx->gj_M, ctx->gj_status};
-    P2G_TRY(gj_invert(ctx, w, static_cast<int>(m), nullptr, nullptr, ctx->coeffs.as<uint16_t>(),
+    P2G_TRY(gj_invert(ctx, w, static_cast<int>(m), nullptr, nullptr, nullptr, ctx->coeffs.as<uint16_t>(),
                       ctx->inv.as<uint16_t>()));
     int singular = 0;
     P2G_TRY(gj_status(ctx, w, &singular));
@@ -698,7 +698,7 @@ int p2g_reconstruction_matrix(p2g_ctx *ctx, size_t k, const uint64_t *missing, s
     P2G_TRY(ctx->inv.ensure(m * m * 2));
     GjWork w{ctx->gj_M, ctx->gj_status};
     P2G_TRY(gj_invert(ctx, w, static_cast<int>(m), reinterpret_cast<const uint16_t *>(dp + L.a_off),
-                      reinterpret_cast<const uint32_t *>(dp + L.b_off), nullptr,
+                      reinterpret_cast<const uint32_t *>(dp + L.b_off), exps, nullptr,
                       ctx->inv.as<uint16_t>()));
     int singular = 0;
     P2G_TRY(gj_status(ctx, w, &singular));
@@ -783,7 +783,7 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
     P2G_TRY(ctx->inv.ensure(m * m * 2));
     GjWork w{ctx->gj_M, ctx->gj_status};
     P2G_TRY(gj_invert(ctx, w, static_cast<int>(m), reinterpret_cast<const uint16_t *>(dp + L.a_off),
-                      d_exps, nullptr, ctx->inv.as<uint16_t>()));
+                      d_exps, exps, nullptr, ctx->inv.as<uint16_t>()));
     int singular = 0;
     P2G_TRY(gj_status(ctx, w, &singular));
     if (singular) {

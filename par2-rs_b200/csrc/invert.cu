@@ -427,13 +427,205 @@ __global__ void gj_extract_perm(const uint16_t *__restrict__ M, int m, int W,
         inv[static_cast<size_t>(c) * m + j] = row[j];
 }
 
+// ---- consecutive exponents: the inverse of a Vandermonde matrix ----------
+//
+// When the recovery exponents are a permutation of s, s+1, ..., s+m-1 (the m
+// lowest exponents of an undamaged recovery set), A[r][j] = x_j^(s + e_r) with
+// x_j the constants of the missing slices, i.e. A = V D with V[e][j] = x_j^e
+// (a transposed Vandermonde matrix) and D = diag(x_j^s).  Row j of V^-1 holds
+// the coefficients of the Lagrange polynomial
+//     L_j(z) = Q_j(z) / Q_j(x_j),   Q_j(z) = P(z) / (z + x_j),   P(z) = prod_k (z + x_k),
+// since L_j(x_k) = [j == k].  So inv[j][r] = x_j^-s coef_{e_r - s}(L_j): O(m^2)
+// work in place of the elimination's O(m^3), and the same matrix (the inverse
+// is unique).  A is singular exactly when two x_j are equal (Q_j(x_j) = 0),
+// or when some x_j = 0 and s > 0; both are reported like a failed
+// elimination.
+
+constexpr uint16_t kNoLog = 0xFFFF;  // log of 0
+
+// level 0 of the product tree: the factors z + x_k (leading 1 implicit)
+__global__ void vdm_leaves(const uint16_t *__restrict__ x, int m, uint16_t *__restrict__ P,
+                           uint16_t *__restrict__ LP, const uint16_t *__restrict__ glog)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) {
+        P[k] = x[k];
+        LP[k] = x[k] ? glog[x[k]] : kNoLog;
+    }
+}
+
+// One level of the product tree.  Pin holds monic polynomials of degree G
+// (the last one shorter), each as its G low coefficients at offset g*G;
+// pairs are multiplied into Pout (degree 2G at offset q*2G).  One thread per
+// output coefficient; LP/LPout are the logs of the coefficients.
+__global__ void vdm_level(const uint16_t *__restrict__ Pin, const uint16_t *__restrict__ LPin,
+                          uint16_t *__restrict__ Pout, uint16_t *__restrict__ LPout, int m, int G,
+                          const uint16_t *__restrict__ glog, const uint16_t *__restrict__ gexp)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m)
+        return;
+    const int base = (t / (2 * G)) * 2 * G, u = t - base;
+    const int a = min(G, m - base), b = max(0, min(G, m - base - G));
+    if (b == 0) {
+        Pout[t] = Pin[t];
+        LPout[t] = LPin[t];
+        return;
+    }
+    // c_u = sum_{i+j=u} A_i B_j with A_a = B_b = 1 (u < a + b)
+    const uint16_t *LA = LPin + base, *LB = LPin + base + G;
+    uint32_t acc = 0;
+    for (int i = max(0, u - b); i <= min(u, a); ++i) {
+        const int j = u - i;
+        const uint32_t la = i == a ? 0u : LA[i], lb = j == b ? 0u : LB[j];
+        if (la != kNoLog && lb != kNoLog) {
+            uint32_t l = la + lb;
+            if (l >= 65535u)
+                l -= 65535u;
+            acc ^= gexp[l];
+        }
+    }
+    Pout[t] = static_cast<uint16_t>(acc);
+    LPout[t] = acc ? glog[acc] : kNoLog;
+}
+
+// y * q for a fixed y given as X[i] = y * 2^i (i < 16): the XOR of the X[i]
+// selected by the bits of q, summed in four independent chains.
+__device__ __forceinline__ uint32_t gmul_fixed(const uint32_t X[16], uint32_t q)
+{
+    uint32_t r[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        r[i & 3] ^= X[i] & (0u - ((q >> i) & 1u));
+    return (r[0] ^ r[1]) ^ (r[2] ^ r[3]);
+}
+
+// Thread j: Q_j = P / (z + x_j) by synthetic division (q_{m-1} = 1,
+// q_{i-1} = p_i + x_j q_i), written transposed (QT[i][j]), and Q_j(x_j) by
+// Horner in the same pass; scale[j] = x_j^-s / Q_j(x_j).
+__global__ void vdm_quotients(const uint16_t *__restrict__ P, const uint16_t *__restrict__ x,
+                              int m, uint32_t s, uint16_t *__restrict__ QT,
+                              uint16_t *__restrict__ scale, int *__restrict__ status,
+                              const uint16_t *__restrict__ glog, const uint16_t *__restrict__ gexp)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m)
+        return;
+    const uint32_t xj = x[j];
+    uint32_t X[16];
+    X[0] = xj;
+#pragma unroll
+    for (int i = 1; i < 16; ++i)
+        X[i] = ((X[i - 1] << 1) ^ ((X[i - 1] & 0x8000u) ? 0x1100Bu : 0u)) & 0xFFFFu;
+    uint32_t q = 1, h = 1;
+    QT[static_cast<size_t>(m - 1) * m + j] = 1;
+    for (int i = m - 1; i >= 1; --i) {
+        q = __ldg(P + i) ^ gmul_fixed(X, q);
+        QT[static_cast<size_t>(i - 1) * m + j] = static_cast<uint16_t>(q);
+        h = gmul_fixed(X, h) ^ q;
+    }
+    if (h == 0 || (xj == 0 && s != 0)) {
+        atomicExch(status, 1);
+        scale[j] = 0;
+        return;
+    }
+    // x_j^-s / h = 2^(-(s log x_j) - log h)  (mod 65535)
+    const uint64_t lx = xj ? glog[xj] : 0;
+    const uint64_t neg = (lx * s + glog[h]) % 65535u;
+    scale[j] = gexp[neg == 0 ? 0 : 65535u - neg];
+}
+
+// inv[j][r] = scale[j] * QT[e_r - s][j], through a 32 x 32 shared-memory tile
+// so that both the reads (along j) and the writes (along r) are coalesced.
+__global__ void vdm_finish(const uint16_t *__restrict__ QT, const uint16_t *__restrict__ scale,
+                           const uint32_t *__restrict__ exps, uint32_t s, int m,
+                           uint16_t *__restrict__ inv, const uint16_t *__restrict__ glog,
+                           const uint16_t *__restrict__ gexp)
+{
+    __shared__ uint16_t tile[32][33];
+    const int j0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int rr = ty; rr < 32; rr += blockDim.y) {
+        const int r = r0 + rr, j = j0 + tx;
+        tile[rr][tx] = (r < m && j < m) ? QT[static_cast<size_t>(exps[r] - s) * m + j] : 0;
+    }
+    __syncthreads();
+    for (int jj = ty; jj < 32; jj += blockDim.y) {
+        const int j = j0 + jj, r = r0 + tx;
+        if (j < m && r < m)
+            inv[static_cast<size_t>(j) * m + r] =
+                static_cast<uint16_t>(gmul(scale[j], tile[tx][jj], glog, gexp));
+    }
+}
+
+// true when exps[0..m) is a permutation of s .. s+m-1
+static bool exps_are_run(const uint32_t *exps, int m, uint32_t *s)
+{
+    uint32_t lo = exps[0], hi = exps[0];
+    for (int r = 1; r < m; ++r) {
+        lo = std::min(lo, exps[r]);
+        hi = std::max(hi, exps[r]);
+    }
+    if (static_cast<uint64_t>(hi) - lo + 1 != static_cast<uint64_t>(m))
+        return false;
+    std::vector<char> seen(m, 0);
+    for (int r = 0; r < m; ++r) {
+        if (seen[exps[r] - lo])
+            return false;
+        seen[exps[r] - lo] = 1;
+    }
+    *s = lo;
+    return true;
+}
+
+static int vdm_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_x, const uint32_t *d_exps,
+                      uint32_t s, uint16_t *d_inv)
+{
+    const size_t vec = (static_cast<size_t>(m) * 2 + 255) & ~static_cast<size_t>(255);
+    P2G_TRY(w.status.ensure(256 + 5 * vec));
+    P2G_TRY(w.M.ensure(static_cast<size_t>(m) * m * 2 + 16));
+    uint8_t *aux = w.status.as<uint8_t>();
+    int *status = reinterpret_cast<int *>(aux);
+    uint16_t *P[2] = {reinterpret_cast<uint16_t *>(aux + 256),
+                      reinterpret_cast<uint16_t *>(aux + 256 + vec)};
+    uint16_t *LP[2] = {reinterpret_cast<uint16_t *>(aux + 256 + 2 * vec),
+                       reinterpret_cast<uint16_t *>(aux + 256 + 3 * vec)};
+    uint16_t *scale = reinterpret_cast<uint16_t *>(aux + 256 + 4 * vec);
+    P2G_CUDA(cudaMemsetAsync(status, 0, sizeof(int), ctx->stream));
+    const int tb = 256, nb = (m + tb - 1) / tb;
+    vdm_leaves<<<nb, tb, 0, ctx->stream>>>(d_x, m, P[0], LP[0], ctx->d_log);
+    P2G_CUDA(cudaGetLastError());
+    ++ctx->launches;
+    int cur = 0;
+    for (int G = 1; G < m; G *= 2) {
+        vdm_level<<<nb, tb, 0, ctx->stream>>>(P[cur], LP[cur], P[cur ^ 1], LP[cur ^ 1], m, G,
+                                              ctx->d_log, ctx->d_exp);
+        P2G_CUDA(cudaGetLastError());
+        ++ctx->launches;
+        cur ^= 1;
+    }
+    uint16_t *QT = w.M.as<uint16_t>();
+    vdm_quotients<<<(m + 31) / 32, 32, 0, ctx->stream>>>(P[cur], d_x, m, s, QT, scale, status,
+                                                         ctx->d_log, ctx->d_exp);
+    P2G_CUDA(cudaGetLastError());
+    ++ctx->launches;
+    const dim3 g2((m + 31) / 32, (m + 31) / 32), b2(32, 8);
+    vdm_finish<<<g2, b2, 0, ctx->stream>>>(QT, scale, d_exps, s, m, d_inv, ctx->d_log, ctx->d_exp);
+    P2G_CUDA(cudaGetLastError());
+    ++ctx->launches;
+    return P2G_OK;
+}
+
 static size_t al256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
 
 int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uint32_t *d_exps,
-              const uint16_t *d_A, uint16_t *d_inv)
+              const uint32_t *h_exps, const uint16_t *d_A, uint16_t *d_inv)
 {
     if (m <= 0)
         return P2G_OK;
+    uint32_t s = 0;
+    if (!d_A && h_exps && exps_are_run(h_exps, m, &s))
+        return vdm_invert(ctx, w, m, d_cmiss, d_exps, s, d_inv);
     const int W = (2 * m + 7) & ~7;  // row stride in u16: rows are 16-byte aligned
     const size_t row_bytes = static_cast<size_t>(W) * 2;
     P2G_TRY(w.M.ensure(static_cast<size_t>(m) * row_bytes));

@@ -13,9 +13,11 @@ struct GjWork {
 // Inverts the m x m matrix given either as PAR2 constants of the missing
 // slices and recovery exponents (A[row][col] = cmiss[col]^exps[row]) or, when
 // d_A is non-null, as a dense row-major device matrix.  d_inv receives A^-1
-// (row-major m x m).  Singularity is reported by gj_status.
+// (row-major m x m).  h_exps (optional) is a host copy of the exponents: when
+// they are a permutation of consecutive values, the closed-form Vandermonde
+// inverse replaces the elimination.  Singularity is reported by gj_status.
 int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uint32_t *d_exps,
-              const uint16_t *d_A, uint16_t *d_inv);
+              const uint32_t *h_exps, const uint16_t *d_A, uint16_t *d_inv);
 
 // Waits for the inversion and reads its status (1 = singular).
 int gj_status(p2g_ctx *ctx, GjWork &w, int *singular);

@@ -24,16 +24,54 @@ def par2_matrix(k, missing, exps):
     return np.array([[oracle.gf_pow(int(c[j]), int(e)) for j in missing] for e in exps], np.uint16)
 
 
+def exponent_set(kind, m, rng):
+    """run: 0..m-1 and offset/perm: a permuted run s..s+m-1 (closed-form
+    Vandermonde inverse); gapped: not consecutive (Gauss-Jordan)."""
+    if kind == "run":
+        return np.arange(m)
+    if kind == "offset":
+        return np.arange(7, 7 + m)
+    if kind == "perm":
+        return rng.permutation(np.arange(3, 3 + m))
+    return np.concatenate([np.arange(m - 1), [m + 4]])
+
+
+@pytest.mark.parametrize("kind", ["run", "offset", "perm", "gapped"])
 @pytest.mark.parametrize("m", [1, 2, 13, 64, 96, 97, 130, 200, 333])
-def test_reconstruction_matrix_matches_oracle(ctx, m):
+def test_reconstruction_matrix_matches_oracle(ctx, m, kind):
     rng = np.random.default_rng(m)
     k = 4 * m + 7
     missing = np.sort(rng.choice(k, m, replace=False))
-    exps = np.arange(m)
+    exps = exponent_set(kind, m, rng)
     got = ctx.reconstruction_matrix(k, missing, exps)
     want = oracle.invert(par2_matrix(k, missing, exps))
     assert want is not None
     assert np.array_equal(got, want)
+
+
+def test_reconstruction_matrix_large_run(ctx):
+    rng = np.random.default_rng(700)
+    k, m = 3000, 700
+    missing = np.sort(rng.choice(k, m, replace=False))
+    exps = np.arange(m)
+    assert np.array_equal(ctx.reconstruction_matrix(k, missing, exps),
+                          oracle.invert(par2_matrix(k, missing, exps)))
+
+
+@pytest.mark.parametrize("kind", ["run", "gapped"])
+def test_repeated_constants_are_singular(ctx, kind):
+    """Beyond 32768 slices the PAR2 constants repeat (c_i = c_{i+32768}):
+    losing both slices of such a pair is unrepairable on either path."""
+    import par2gpu
+
+    k = 40000
+    c = oracle.par2_constants(k)
+    assert c[5] == c[5 + 32768]
+    missing = np.array([5, 9, 5 + 32768])
+    exps = np.arange(3) if kind == "run" else np.array([0, 1, 3])
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        ctx.reconstruction_matrix(k, missing, exps)
+    assert ei.value.code == par2gpu.ESINGULAR
 
 
 def test_invert_random_and_singular(ctx):
