@@ -217,13 +217,16 @@ def run_ours(args, rank, world):
             dist.barrier()
 
     def max_over_ranks(v):
-        if world > 1:
-            t = torch.tensor([v], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return v
+        from par2gpu.shard import max_over_ranks as mx
+
+        return mx(v, device=dev)
 
     # ---- device-resident timed region (value) ----
+    # A set larger than L2 (126 MB) streams from HBM on every step; a smaller
+    # one is evicted between steps by writing a 256 MiB buffer, outside the
+    # per-step events.
+    big = (k + r) * S > (256 << 20)
+    flush = None if big else torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     for _ in range(args.warmup):
         step_dev()
     ctx.set_timing(True)
@@ -231,20 +234,22 @@ def run_ours(args, rank, world):
     barrier()
     torch.cuda.synchronize(dev)
     clocks.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
     mul_ms, launches = [], 0
-    for _ in range(args.steps):
+    for a, b in evs:
+        if flush is not None:
+            flush.fill_(1)
+        a.record(stream)
         step_dev()
+        b.record(stream)
         t = ctx.last_timing()
         mul_ms.append(t.ms_kernel)
         launches += t.launches
-    ev1.record(stream)
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
     barrier()
-    ms_step = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    ms_step = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs) / args.steps)
     ctx.set_timing(False)
     value = world * k * S / (ms_step * 1e-3) / 1e9
 
@@ -296,7 +301,8 @@ def run_ours(args, rank, world):
         "alg_bytes": alg_bytes,
         "hbm": {"achieved": alg_bytes / t_kernel / 1e9, "peak": hbm_peak, "unit": "GB/s",
                 "frac": alg_bytes / t_kernel / 1e9 / hbm_peak, "peak_source": peak_kind},
-        "traffic": traffic_from_profile(),
+        # ncu DRAM bytes per launch, profiled for the large-encode shape only
+        "traffic": traffic_from_profile() if WORKLOAD == WORKLOADS["large_encode"][3] else None,
     }
 
     # ---- CPU baseline + bit-exact cross-check on the same column sample ----
@@ -321,7 +327,8 @@ def run_ours(args, rank, world):
             "config": {"workload": WORKLOAD, "k": k, "r": r, "slice_bytes": S,
                        "plan": plan if plan else "heuristic",
                        "parallelism": f"{world} independent sets" if world > 1 else "1 set",
-                       "l2": "inputs 2 GiB per step > 126 MB L2; no flush"},
+                       "l2": (f"inputs {(k + r) * S / 2**20:.0f} MiB per step > 126 MB L2; no flush"
+                              if big else "L2 flushed between steps (256 MiB write, untimed)")},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GB/s", "ms_per_step": e2e_ms,
@@ -426,6 +433,58 @@ def run_verify_repair(args):
                      "int_roofline_frac": (2.0 * macs / (tot * 1e-3)) / int_peak if int_peak else None}
     ctx.close()
     print(json.dumps(out), flush=True)
+
+
+HASH_WORKLOADS = {
+    # the IFSC checksums of the verify configuration
+    "hash": (32000, 64 << 10, "hash: MD5+CRC32 of 32000 x 64 KiB seeded uniform slices"),
+    # the same occupancy (256 slices on each of 148 SMs) at 310 MB, for ncu
+    "profile_hash": (37888, 8 << 10, "profile_hash: MD5+CRC32 of 37888 x 8 KiB seeded uniform "
+                                     "slices"),
+}
+
+
+def run_hash(args):
+    """Per-slice MD5 + CRC32 of device-resident slices; roofline in integer
+    ops (MD5: 64 steps x 5 ops per 64-byte block; CRC32 counted as bytes)."""
+    import torch
+
+    import par2gpu
+
+    n, S, name = HASH_WORKLOADS[args.workload]
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED)
+    d = torch.randint(0, 256, (n, S), dtype=torch.uint8, device=dev, generator=g)
+    ptrs = [d.data_ptr() + i * S for i in range(n)]
+    ctx = par2gpu.Context(0)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    for _ in range(args.warmup):
+        ctx.hash_slices(ptrs, S, device=True)
+    ctx.set_timing(True)
+    ker, tot = [], []
+    for _ in range(max(1, args.steps)):
+        md5, crc = ctx.hash_slices(ptrs, S, device=True)
+        t = ctx.last_timing()
+        ker.append(t.ms_kernel)
+        tot.append(t.ms_total)
+    ctx.close()
+    # the first and last slices against the oracle
+    from oracle import oracle
+
+    host = d[[0, n - 1]].cpu().numpy()
+    wmd5, wcrc = oracle.hash_slices(host)
+    ok = bool(np.array_equal(md5[[0, n - 1]], wmd5) and np.array_equal(crc[[0, n - 1]], wcrc))
+    int_peak, sms = probe_int_peak(0)
+    kms = statistics.median(ker)
+    ops = n * S / 64 * 64 * 5
+    print(json.dumps({"workload": name, "slices": n, "slice_bytes": S, "steps": args.steps,
+                      "kernel_ms": kms, "call_ms": statistics.median(tot),
+                      "gbs": n * S / kms / 1e6,
+                      "roofline": {"bound": "int", "achieved": ops / kms / 1e9,
+                                   "peak": (int_peak or 0) / 1e12, "unit": "Tops/s (MD5 5 ops/step)",
+                                   "frac": ops / (kms * 1e-3) / int_peak if int_peak else None},
+                      "matches_oracle": ok}), flush=True)
 
 
 def batched_sets(seed, nsets=256):
@@ -702,12 +761,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large_encode",
-                    choices=sorted(WORKLOADS) + ["verify_repair", "batched", "serving"])
+                    choices=sorted(WORKLOADS) + sorted(HASH_WORKLOADS) +
+                    ["verify_repair", "batched", "serving"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the heuristic tile shape instead of the autotuned one")
     ap.add_argument("--quick", action="store_true",
                     help="device-resident timing only (no e2e, roofline probe or CPU baseline)")
     args = ap.parse_args()
+    if args.workload in HASH_WORKLOADS:
+        run_hash(args)
+        return
     if args.workload == "verify_repair":
         run_verify_repair(args)
         return
