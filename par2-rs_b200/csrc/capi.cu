@@ -120,6 +120,36 @@ static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 
 // 16-byte aligned are used in place; host pointers (or misaligned device
 // pointers) are staged through `buf` (one padded slot per slice).  `copy_in`
 // copies the current contents in.
+// Copies n slices of `bytes` each, src[i] -> dst[i], on `stream`.  Runs of
+// slices whose source and destination addresses both advance by constant
+// strides (slices cut from one buffer) become one 2D copy: one DMA transfer
+// instead of one per slice.
+static int copy_slices(uint8_t *const *dst, const uint8_t *const *src, size_t n, size_t bytes,
+                       cudaMemcpyKind kind, cudaStream_t stream)
+{
+    constexpr ptrdiff_t kMaxPitch = ptrdiff_t(1) << 30;
+    size_t i = 0;
+    while (i < n) {
+        size_t j = i + 1;
+        if (j < n) {
+            const ptrdiff_t hs = src[j] - src[i], ds = dst[j] - dst[i];
+            if (hs >= static_cast<ptrdiff_t>(bytes) && ds >= static_cast<ptrdiff_t>(bytes) &&
+                hs <= kMaxPitch && ds <= kMaxPitch) {
+                while (j + 1 < n && src[j + 1] - src[j] == hs && dst[j + 1] - dst[j] == ds)
+                    ++j;
+                ++j;  // [i, j) has constant strides
+                P2G_CUDA(cudaMemcpy2DAsync(dst[i], static_cast<size_t>(ds), src[i],
+                                           static_cast<size_t>(hs), bytes, j - i, kind, stream));
+                i = j;
+                continue;
+            }
+        }
+        P2G_CUDA(cudaMemcpyAsync(dst[i], src[i], bytes, kind, stream));
+        ++i;
+    }
+    return P2G_OK;
+}
+
 static int stage(p2g_ctx *ctx, p2g::DevBuf &buf, const uint8_t *const *ptrs, size_t n,
                  size_t bytes, bool device, bool copy_in, std::vector<uint8_t *> &out,
                  bool &staged)
@@ -138,24 +168,20 @@ static int stage(p2g_ctx *ctx, p2g::DevBuf &buf, const uint8_t *const *ptrs, siz
     }
     size_t slot = round16(bytes);
     P2G_TRY(buf.ensure(slot * (n ? n : 1)));
-    for (size_t i = 0; i < n; ++i) {
+    for (size_t i = 0; i < n; ++i)
         out[i] = buf.as<uint8_t>() + i * slot;
-        if (copy_in)
-            P2G_CUDA(cudaMemcpyAsync(out[i], ptrs[i], bytes,
-                                     device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                     ctx->stream));
-    }
+    if (copy_in)
+        P2G_TRY(copy_slices(out.data(), ptrs, n, bytes,
+                            device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            ctx->stream));
     return P2G_OK;
 }
 
 static int unstage(p2g_ctx *ctx, uint8_t *const *user, const std::vector<uint8_t *> &dev,
                    size_t n, size_t bytes, bool device)
 {
-    for (size_t i = 0; i < n; ++i)
-        P2G_CUDA(cudaMemcpyAsync(user[i], dev[i], bytes,
-                                 device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                                 ctx->stream));
-    return P2G_OK;
+    return copy_slices(user, dev.data(), n, bytes,
+                       device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream);
 }
 
 // Starts a call: resets the launch counter and the timing marks.
@@ -530,9 +556,8 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
         P2G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ev[0], 0));
         for (int g = 0; g < groups; ++g) {
             const size_t i0 = k * g / groups, i1 = k * (g + 1) / groups;
-            for (size_t i = i0; i < i1; ++i)
-                P2G_CUDA(cudaMemcpyAsync(s[i], src[i], slice_bytes, cudaMemcpyHostToDevice,
-                                         ctx->copy_stream));
+            P2G_TRY(copy_slices(s.data() + i0, src + i0, i1 - i0, slice_bytes,
+                                cudaMemcpyHostToDevice, ctx->copy_stream));
             P2G_CUDA(cudaEventRecord(ctx->pipe_ev[g], ctx->copy_stream));
             P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
             P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
@@ -756,12 +781,10 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
     const size_t slot = round16(slice_bytes);
     P2G_TRY(ctx->rhs.ensure(slot * m));
     std::vector<uint8_t *> rhs(m);
-    for (size_t j = 0; j < m; ++j) {
+    for (size_t j = 0; j < m; ++j)
         rhs[j] = ctx->rhs.as<uint8_t>() + j * slot;
-        P2G_CUDA(cudaMemcpyAsync(rhs[j], recovery[j], slice_bytes,
-                                 dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                 ctx->stream));
-    }
+    P2G_TRY(copy_slices(rhs.data(), recovery, m, slice_bytes,
+                        dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     P2G_TRY(stage(ctx, ctx->out_copy, out, m, slice_bytes, dev, false, os, o_st));
     // parameter block: [present ptrs][rhs ptrs | out ptrs][cmiss | exps | cpres]
     ParamLayout L(np, 2 * m, m * 2 + m * 4 + 16, np * 2);

@@ -58,7 +58,7 @@ struct p2g_ctx {
     cudaStream_t stream = nullptr;      // where work runs (own or caller's)
     // host-to-device copies that overlap the kernels (p2g_encode from host)
     cudaStream_t copy_stream = nullptr;
-    static constexpr int kPipe = 8;
+    static constexpr int kPipe = 16;
     cudaEvent_t pipe_ev[kPipe] = {};
     std::mutex mu;
     // optional per-phase timing (p2g_set_timing / p2g_last_timing)
