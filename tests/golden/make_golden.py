@@ -12,7 +12,13 @@ establishes it):
 
   * the slice size and every file's name, length and contents (zlib+base64);
   * every file's IFSC entries (MD5, CRC32 of each zero-padded slice);
-  * every recovery slice: exponent and body (zlib+base64).
+  * every recovery slice: exponent and body (zlib+base64);
+  * every distinct packet of the .par2 files (its 64-byte header and, except
+    for RecvSlic packets, whose body is the recovery slice above behind its
+    4-byte exponent, its body) and every .par2 file as the list of its packets
+    in file order, so that a test can rebuild each file byte for byte
+    (checked here against the file) and compare the packets a writer produces
+    header by header.
 
 Packets are parsed with the PAR2 header layout of par2-rs writer.rs:92-123
 (magic, u64 length, packet MD5 over set-id+type+body, set id, type, body) and
@@ -56,6 +62,19 @@ def packets(buf):
         pos += length
 
 
+def packet_list(buf):
+    """(offset, header, type, body) of every valid packet, in file order."""
+    pos, out = 0, []
+    for ptype, body in packets(buf):
+        pos = buf.find(MAGIC, pos)
+        while hashlib.md5(buf[pos + 32:pos + 64] + buf[pos + 64:pos + 64 + len(body)]).digest() \
+                != buf[pos + 16:pos + 32]:
+            pos = buf.find(MAGIC, pos + 1)
+        out.append((pos, buf[pos:pos + 64], ptype, body))
+        pos += 64 + len(body)
+    return out
+
+
 def pack(b):
     return base64.b64encode(zlib.compress(bytes(b), 9)).decode()
 
@@ -96,12 +115,35 @@ def main(src_dir, out_path):
                       "ifsc": ifsc[fid], "data": pack(data)})
     recovery = [{"exponent": e, "body": pack(recv[e]),
                  "md5": hashlib.md5(recv[e]).hexdigest()} for e in sorted(recv)]
+    par2_files, unique, index = [], [], {}
+    for path in sorted(glob.glob(os.path.join(src_dir, "testdata*.par2"))):
+        buf = open(path, "rb").read()
+        plist, rebuilt = [], b""
+        for off, hdr, ptype, body in packet_list(buf):
+            assert off == len(rebuilt), (path, off)  # packets are contiguous
+            if hdr not in index:  # the header's MD5 covers the body
+                ent = {"header": hdr.hex()}
+                if ptype == T_RECV:
+                    (exp,) = struct.unpack_from("<I", body, 0)
+                    assert body[4:] == recv[exp]
+                    ent["exponent"] = exp
+                else:
+                    ent["body"] = pack(body)
+                index[hdr] = len(unique)
+                unique.append(ent)
+            plist.append(index[hdr])
+            rebuilt += hdr + body
+        assert rebuilt == buf, path
+        par2_files.append({"name": os.path.basename(path), "size": len(buf),
+                           "md5": hashlib.md5(buf).hexdigest(), "packets": plist})
     doc = {"source": "par2-rs tests/data (QuickPar 0.4 set testdata.par2 + volumes)",
-           "block_size": block_size, "files": files, "recovery": recovery}
+           "block_size": block_size, "files": files, "recovery": recovery,
+           "par2_packets": unique, "par2_files": par2_files}
     with open(out_path, "w") as f:
         json.dump(doc, f, indent=1)
     print(f"wrote {out_path}: block_size={block_size} files={len(files)} "
-          f"slices={sum(len(f['ifsc']) for f in files)} recovery={len(recovery)}")
+          f"slices={sum(len(f['ifsc']) for f in files)} recovery={len(recovery)} "
+          f"par2 files={len(par2_files)}")
 
 
 if __name__ == "__main__":

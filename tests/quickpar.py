@@ -1,7 +1,9 @@
 """Loader for the golden QuickPar vectors in tests/golden/quickpar.json."""
 import base64
+import hashlib
 import json
 import os
+import struct
 import zlib
 
 import numpy as np
@@ -23,6 +25,34 @@ class QuickParSet:
         self.recovery = {r["exponent"]: np.frombuffer(_unpack(r["body"]), np.uint8)
                          for r in doc["recovery"]}
         self.recovery_md5 = {r["exponent"]: r["md5"] for r in doc["recovery"]}
+        self.packets = []
+        for p in doc.get("par2_packets", []):
+            hdr = bytes.fromhex(p["header"])
+            if "exponent" in p:
+                body = struct.pack("<I", p["exponent"]) + self.recovery[p["exponent"]].tobytes()
+            else:
+                body = _unpack(p["body"])
+            self.packets.append((hdr, body))
+        self.par2_files = doc.get("par2_files", [])
+
+    def par2_bytes(self, name):
+        """The QuickPar .par2 file `name`, rebuilt byte for byte."""
+        for f in self.par2_files:
+            if f["name"] == name:
+                buf = b"".join(self.packets[i][0] + self.packets[i][1] for i in f["packets"])
+                assert len(buf) == f["size"] and hashlib.md5(buf).hexdigest() == f["md5"]
+                return buf
+        raise KeyError(name)
+
+    def materialize(self, d):
+        """Writes the data files and the seven .par2 files of the set into d."""
+        for f in self.files:
+            with open(os.path.join(d, f["name"]), "wb") as o:
+                o.write(f["data"])
+        for f in self.par2_files:
+            with open(os.path.join(d, f["name"]), "wb") as o:
+                o.write(self.par2_bytes(f["name"]))
+        return d
 
     def slices(self, files=None):
         """Zero-padded input slices in canonical order: uint8 [k, block_size],

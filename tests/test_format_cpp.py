@@ -1,0 +1,162 @@
+"""The PAR2 on-disk format (par2-rs_b200/host/par2_format.hpp, driven by
+tests/cpp/test_format.cpp) against the QuickPar fixture set bundled with
+par2-rs: the parser reads the set as par2-rs does (parser.rs:181-800), the
+writer's packets are byte-identical to QuickPar's (every header holds the MD5
+of its body), the files follow par2-rs's layout and names (creator.rs:453-521,
+volumes.rs:65-210), and a created set repairs damaged files."""
+import json
+import os
+import shutil
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests import quickpar
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BIN = os.path.join(HERE, "cpp", "_build", "test_format")
+MAGIC = b"PAR2\x00PKT"
+T_CREATOR = b"PAR 2.0\x00Creator\x00"
+T_MAIN = b"PAR 2.0\x00Main\x00\x00\x00\x00"
+T_DESC = b"PAR 2.0\x00FileDesc"
+T_IFSC = b"PAR 2.0\x00IFSC\x00\x00\x00\x00"
+T_RECV = b"PAR 2.0\x00RecvSlic"
+
+
+def run(*args, check=True):
+    subprocess.run(["make", "-s", "-C", os.path.join(HERE, "cpp")], check=True)
+    p = subprocess.run([BIN, *map(str, args)], capture_output=True, text=True, timeout=600)
+    if check:
+        assert p.returncode == 0, p.stdout + p.stderr
+    return p
+
+
+def packet_headers(buf):
+    """(type, header, exponent or None) of the packets of a file, in order."""
+    out, pos = [], 0
+    while pos + 64 <= len(buf):
+        assert buf[pos:pos + 8] == MAGIC, pos
+        (n,) = struct.unpack_from("<Q", buf, pos + 8)
+        t = buf[pos + 48:pos + 64]
+        e = struct.unpack_from("<I", buf, pos + 64)[0] if t == T_RECV else None
+        out.append((t, buf[pos:pos + 64], e))
+        pos += n
+    assert pos == len(buf)
+    return out
+
+
+@pytest.fixture
+def qp(tmp_path):
+    q = quickpar.load()
+    q.materialize(str(tmp_path))
+    return q, tmp_path
+
+
+def test_parse_quickpar_set(qp):
+    q, d = qp
+    p = json.loads(run("parse", d / "testdata.par2").stdout)
+    assert p["block_size"] == q.block_size
+    assert [f["name"] for f in p["files"]] == [f["name"] for f in q.files]  # Main order
+    for f, g in zip(p["files"], q.files):
+        assert (f["file_id"], f["length"], f["md5"], f["md5_16k"]) == \
+            (g["file_id"], g["length"], g["md5"], g["md5_16k"])
+        assert f["ifsc"] == g["ifsc"]
+    # every volume's recovery slices, found by recovery set ID
+    rec = dict(p["recovery"])
+    assert sorted(rec) == list(range(60))
+    assert all(rec[e] == q.recovery_md5[e] for e in rec)
+
+
+def test_parser_skips_corrupt_packets_and_garbage(qp):
+    q, d = qp
+    buf = bytearray(open(d / "testdata.par2", "rb").read())
+    hdrs = packet_headers(bytes(buf))
+    # flip a byte inside the first IFSC body; insert garbage after the first packet
+    off = 0
+    for t, h, _ in hdrs:
+        if t == T_IFSC:
+            break
+        off += struct.unpack_from("<Q", h, 8)[0]
+    bad_id = bytes(buf[off + 64:off + 80]).hex()
+    buf[off + 100] ^= 0xFF
+    (n0,) = struct.unpack_from("<Q", hdrs[0][1], 8)
+    buf[n0:n0] = b"PAR2\x00PK" + bytes(range(37))
+    open(d / "testdata.par2", "wb").write(bytes(buf))
+    p = json.loads(run("parse", d / "testdata.par2").stdout)
+    assert [f["name"] for f in p["files"]] == [f["name"] for f in q.files]
+    for f, g in zip(p["files"], q.files):
+        assert f["ifsc"] == ([] if f["file_id"] == bad_id else g["ifsc"])
+
+
+def test_main_and_file_desc_packets_match_quickpar(qp):
+    q, d = qp
+    got = [bytes.fromhex(x) for x in
+           run("headers", d, q.block_size, *[f["name"] for f in q.files]).stdout.split()]
+    fixture = {h for h, _ in q.packets}
+    assert len(got) == 11 and all(h in fixture for h in got)
+
+
+def test_missing_input_rejected(tmp_path):
+    p = run("create", tmp_path / "x.par2", 0, 5, "exp", tmp_path / "missing.bin", check=False)
+    assert p.returncode == 1 and "Input file does not exist" in p.stderr
+
+
+@pytest.mark.gpu
+def test_create_writes_quickpar_packets_in_par2_rs_layout(qp, tmp_path):
+    """The QuickPar set recreated (same files, 5376-byte slices, 60 recovery
+    slices): every packet but the Creator is byte-identical to QuickPar's,
+    and the files are those par2-rs writes."""
+    q, src = qp
+    out = tmp_path / "out"
+    out.mkdir()
+    for f in q.files:
+        shutil.copy(src / f["name"], out / f["name"])
+    written = run("create", out / "testdata.par2", q.block_size, 30, "exp",
+                  *[out / f["name"] for f in q.files]).stdout.split()
+    names = sorted(os.path.basename(w) for w in written)
+    assert names == sorted(f["name"] for f in q.par2_files)
+    fixture = {h for h, _ in q.packets}
+    want_exps = {"testdata.par2": []}
+    for n in names[1:]:
+        a, c = n[len("testdata.vol"):-len(".par2")].split("+")
+        want_exps[n] = list(range(int(a), int(a) + int(c)))
+    for w in written:
+        hdrs = packet_headers(open(w, "rb").read())
+        types = [t for t, _, _ in hdrs]
+        nrec = len(want_exps[os.path.basename(w)])
+        assert types == [T_CREATOR, T_MAIN] + [T_DESC] * 10 + [T_IFSC] * 10 + [T_RECV] * nrec
+        assert [e for _, _, e in hdrs if e is not None] == want_exps[os.path.basename(w)]
+        for t, h, _ in hdrs[1:]:
+            assert h in fixture, (os.path.basename(w), t)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheme", ["single", "exp"])
+def test_create_damage_repair_roundtrip(tmp_path, scheme):
+    rng = np.random.default_rng(11)
+    names = []
+    for i, n in enumerate([0, 1, 4096, 10000, 65536, 123457, 300001]):
+        name = f"file{i}.bin"
+        (tmp_path / name).write_bytes(rng.integers(0, 256, n, dtype=np.uint8).tobytes())
+        names.append(name)
+    orig = {n: (tmp_path / n).read_bytes() for n in names}
+    # 126 slices of 4096 bytes, 20 %: 26 recovery slices
+    written = run("create", tmp_path / "set.par2", 4096, 20, scheme,
+                  *[tmp_path / n for n in names]).stdout.split()
+    assert os.path.basename(written[0]) == "set.par2"
+    p = json.loads(run("parse", tmp_path / "set.par2").stdout)
+    assert sorted(f["name"] for f in p["files"]) == sorted(names)
+    assert p["block_size"] == 4096
+    # lose one file, damage three slices of another
+    os.unlink(tmp_path / "file4.bin")
+    b = bytearray(orig["file6.bin"])
+    for off in (5, 4096 * 20 + 7, len(b) - 1):
+        b[off] ^= 0x5A
+    (tmp_path / "file6.bin").write_bytes(bytes(b))
+    r = run("repair", tmp_path / "set.par2", tmp_path).stdout.split("\n")
+    assert r[0] == "damaged 19" and r[1] == "repaired 19"
+    for n in names:
+        assert (tmp_path / n).read_bytes() == orig[n], n
+    assert run("repair", tmp_path / "set.par2", tmp_path).stdout.split("\n")[0] == "damaged 0"
