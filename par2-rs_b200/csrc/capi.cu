@@ -114,12 +114,10 @@ static int upload_params(p2g_ctx *ctx, const ParamLayout &L)
     return P2G_OK;
 }
 
+constexpr int kTailSlabs = 4;  // column slabs of the last input group (host outputs)
+
 static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-// Resolves the slice pointers a kernel will use: device pointers that are
-// 16-byte aligned are used in place; host pointers (or misaligned device
-// pointers) are staged through `buf` (one padded slot per slice).  `copy_in`
-// copies the current contents in.
 // Copies n slices of `bytes` each, src[i] -> dst[i], on `stream`.  Runs of
 // slices whose source and destination addresses both advance by constant
 // strides (slices cut from one buffer) become one 2D copy: one DMA transfer
@@ -150,6 +148,10 @@ static int copy_slices(uint8_t *const *dst, const uint8_t *const *src, size_t n,
     return P2G_OK;
 }
 
+// Resolves the slice pointers a kernel will use: device pointers that are
+// 16-byte aligned are used in place; host pointers (or misaligned device
+// pointers) are staged through `buf` (one padded slot per slice).  `copy_in`
+// copies the current contents in.
 static int stage(p2g_ctx *ctx, p2g::DevBuf &buf, const uint8_t *const *ptrs, size_t n,
                  size_t bytes, bool device, bool copy_in, std::vector<uint8_t *> &out,
                  bool &staged)
@@ -530,7 +532,16 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     bool s_staged = false, d_staged = false;
     P2G_TRY(stage(ctx, ctx->in_copy, src, k, slice_bytes, dev, groups == 1, s, s_staged));
     P2G_TRY(stage(ctx, ctx->out_copy, out, r, slice_bytes, dev, false, d, d_staged));
-    ParamLayout L(k, r, k * 2, r * 4);
+    // With host outputs, the last input group runs as column slabs: the
+    // outputs of a finished slab go back while the next slab computes.
+    const size_t tiles = (slice_bytes + 2047) / 2048;
+    const int slabs = (groups > 1 && d_staged && tiles >= 32) ? kTailSlabs : 1;
+    const size_t last0 = k * (groups - 1) / groups, nlast = k - last0;
+    std::vector<size_t> cut(slabs + 1);
+    for (int q = 0; q <= slabs; ++q)
+        cut[q] = q == slabs ? slice_bytes : tiles * q / slabs * 2048;
+    const size_t tail_bytes = slabs > 1 ? slabs * (nlast + r) * sizeof(void *) : 0;
+    ParamLayout L(k, r, k * 2, round16(r * 4) + tail_bytes);
     P2G_TRY(ctx->hparams.ensure(L.total));
     P2G_TRY(ctx->params.ensure(L.total));
     uint8_t *h = ctx->hparams.as<uint8_t>();
@@ -538,6 +549,17 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     memcpy(h + L.dst_off, d.data(), r * sizeof(void *));
     par2_constants(k, reinterpret_cast<uint16_t *>(h + L.a_off));
     memcpy(h + L.b_off, exps, r * 4);
+    const size_t tail_off = L.b_off + round16(r * 4);
+    if (slabs > 1) {
+        // per slab: the last group's inputs, then the outputs, offset to the slab
+        uint8_t **t = reinterpret_cast<uint8_t **>(h + tail_off);
+        for (int q = 0; q < slabs; ++q) {
+            for (size_t i = 0; i < nlast; ++i)
+                *t++ = s[last0 + i] + cut[q];
+            for (size_t e = 0; e < r; ++e)
+                *t++ = d[e] + cut[q];
+        }
+    }
     P2G_TRY(upload_params(ctx, L));
     uint8_t *dp = ctx->params.as<uint8_t>();
     P2G_TRY(ctx->recs.ensure(k * r * 64));
@@ -560,12 +582,36 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
                                 cudaMemcpyHostToDevice, ctx->copy_stream));
             P2G_CUDA(cudaEventRecord(ctx->pipe_ev[g], ctx->copy_stream));
             P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
-            P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
-                               static_cast<int>(r), slice_bytes,
-                               ctx->recs.as<uint32_t>() + i0 * r * 16, g == 0 ? 0 : 1));
+            if (g < groups - 1 || slabs == 1) {
+                P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
+                                   static_cast<int>(r), slice_bytes,
+                                   ctx->recs.as<uint32_t>() + i0 * r * 16, g == 0 ? 0 : 1));
+                continue;
+            }
+            // the last group, slab by slab; each slab's outputs go back on the
+            // copy stream (its uploads are done) as soon as the slab is final
+            uint8_t *const *tab = reinterpret_cast<uint8_t *const *>(dp + tail_off);
+            std::vector<uint8_t *> uo(r), so(r);
+            for (int q = 0; q < slabs; ++q) {
+                const uint8_t *const *qs = reinterpret_cast<const uint8_t *const *>(tab + q * (nlast + r));
+                P2G_TRY(muladd_run(ctx, qs, static_cast<int>(nlast), tab + q * (nlast + r) + nlast,
+                                   static_cast<int>(r), cut[q + 1] - cut[q],
+                                   ctx->recs.as<uint32_t>() + i0 * r * 16, 1));
+                P2G_CUDA(cudaEventRecord(ctx->pipe_ev[q], ctx->stream));
+                P2G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ev[q], 0));
+                for (size_t e = 0; e < r; ++e) {
+                    uo[e] = out[e] + cut[q];
+                    so[e] = d[e] + cut[q];
+                }
+                P2G_TRY(copy_slices(uo.data(), so.data(), r, cut[q + 1] - cut[q],
+                                    cudaMemcpyDeviceToHost, ctx->copy_stream));
+            }
+            // the call ends when the last read-back has landed
+            P2G_CUDA(cudaEventRecord(ctx->pipe_ev[slabs], ctx->copy_stream));
+            P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[slabs], 0));
         }
     }
-    if (d_staged)
+    if (d_staged && slabs == 1)
         P2G_TRY(unstage(ctx, out, d, r, slice_bytes, dev));
     return finish(ctx);
 }

@@ -72,6 +72,23 @@ def test_encode_matches_oracle(ctx, k, S, r):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("k,S,r", [(128, 65536, 9), (300, 65536 + 2050, 7), (200, 131072 + 4, 30)])
+def test_host_pipeline_groups_and_tail_slabs(ctx, k, S, r):
+    """Host buffers with k >= 128: inputs go up in groups while earlier groups
+    are accumulated, and the last group runs as column slabs whose outputs go
+    back while the next slab computes (ragged last slab included)."""
+    rng = np.random.default_rng(k + S)
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(r, dtype=np.uint32)
+    want = oracle.encode(src, exps)
+    assert np.array_equal(ctx.encode_array(src, exps), want)
+    # separately allocated rows (no common stride): one copy per slice
+    rows = [np.ascontiguousarray(src[i]) for i in range(k)]
+    outs = [np.zeros(S, np.uint8) for _ in range(r)]
+    ctx.encode(rows, S, exps, outs)
+    assert np.array_equal(np.stack(outs), want)
+
+
 def test_encode_sparse_exponents_and_zero_slices(ctx):
     rng = np.random.default_rng(5)
     src = rng.integers(0, 256, (30, 4096), dtype=np.uint8)
