@@ -95,12 +95,46 @@ constexpr int kSmallM = 96;   // matrices up to this size: one CTA, all in share
 constexpr int kPanel = 64;    // panel width of the blocked elimination
 constexpr int kGjThreads = 256;
 
+constexpr uint32_t kLogZero = 0xFFFFu;  // marks log(0)
+
+__device__ __forceinline__ uint32_t glog_or_zero(uint32_t v, const uint16_t *__restrict__ glog)
+{
+    return v ? __ldg(glog + v) : kLogZero;
+}
+
+// product from logs (either kLogZero: 0) with the antilog table in shared memory
+__device__ __forceinline__ uint32_t gmul_logs_s(uint32_t la, uint32_t lb, const uint16_t *sexp)
+{
+    if (la == kLogZero || lb == kLogZero)
+        return 0;
+    uint32_t l = la + lb;
+    if (l >= 65535u)
+        l -= 65535u;
+    return sexp[l];
+}
+
+constexpr size_t kExpSmem = 65535 * sizeof(uint16_t);  // antilog table in shared memory
+
+// Copies the antilog table into shared memory (all threads; ends with a barrier).
+__device__ void load_exp_table(uint16_t *sexp, const uint16_t *__restrict__ gexp)
+{
+    const uint32_t *g = reinterpret_cast<const uint32_t *>(gexp);
+    uint32_t *d = reinterpret_cast<uint32_t *>(sexp);
+    for (int i = threadIdx.x; i < 65535 / 2; i += blockDim.x)
+        d[i] = __ldg(g + i);
+    if (threadIdx.x == 0)
+        sexp[65534] = gexp[65534];
+    __syncthreads();
+}
+
 // Gauss-Jordan on [A | I] (n x 2n, row stride ld) in shared memory by one
 // CTA, with the reference's pivot rule: rows are swapped only when the
 // diagonal entry is zero (first non-zero row below).  Returns false (for every
-// thread) when A is singular.
-__device__ bool cta_gauss_jordan(uint16_t *S, int n, int ld, uint32_t *fcol,
-                                 const uint16_t *__restrict__ glog,
+// thread) when A is singular.  Each elimination step takes the logs of the
+// pivot row (lrow, 2n entries) and of the row factors (fcol) once, so every
+// product of the row updates is one lookup in the shared antilog table sexp.
+__device__ bool cta_gauss_jordan(uint16_t *S, int n, int ld, uint32_t *fcol, uint32_t *lrow,
+                                 const uint16_t *sexp, const uint16_t *__restrict__ glog,
                                  const uint16_t *__restrict__ gexp)
 {
     __shared__ int piv;
@@ -134,19 +168,30 @@ __device__ bool cta_gauss_jordan(uint16_t *S, int n, int ld, uint32_t *fcol,
             }
             __syncthreads();
         }
+        // scale the pivot row by 1/pivot and keep the logs of its entries
         const uint32_t pinv = ginv(S[k * ld + k], glog, gexp);
         __syncthreads();
-        for (int j = tid; j < w2; j += nt)
-            S[k * ld + j] = static_cast<uint16_t>(gmul_alu(S[k * ld + j], pinv));
-        __syncthreads();
+        for (int j = tid; j < w2; j += nt) {
+            const uint32_t v = gmul_alu(S[k * ld + j], pinv);
+            S[k * ld + j] = static_cast<uint16_t>(v);
+            lrow[j] = glog_or_zero(v, glog);
+        }
         for (int r = tid; r < n; r += nt)
-            fcol[r] = r == k ? 0u : S[r * ld + k];
+            fcol[r] = r == k ? kLogZero : glog_or_zero(S[r * ld + k], glog);
         __syncthreads();
-        for (int idx = tid; idx < n * w2; idx += nt) {
-            const int r = idx / w2, j = idx - r * w2;
-            const uint32_t f = fcol[r];
-            if (f)
-                S[r * ld + j] ^= static_cast<uint16_t>(gmul_alu(f, S[k * ld + j]));
+        // S[r][j] ^= f_r * S[k][j] over the n x 2n block, no division per entry
+        int r = tid / w2, j = tid - r * w2;
+        const int dr = nt / w2, dj = nt - dr * w2;
+        for (; r < n;) {
+            const uint32_t lf = fcol[r];
+            if (lf != kLogZero)
+                S[r * ld + j] ^= static_cast<uint16_t>(gmul_logs_s(lf, lrow[j], sexp));
+            r += dr;
+            j += dj;
+            if (j >= w2) {
+                j -= w2;
+                ++r;
+            }
         }
         __syncthreads();
     }
@@ -159,14 +204,17 @@ __global__ void __launch_bounds__(kGjThreads)
              int *__restrict__ status, const uint16_t *__restrict__ glog,
              const uint16_t *__restrict__ gexp)
 {
-    extern __shared__ uint16_t S[];  // m x 2m
+    extern __shared__ __align__(16) uint16_t dyn[];  // antilog table, then S (m x 2m)
+    uint16_t *sexp = dyn, *S = dyn + 65536;
     __shared__ uint32_t fcol[kSmallM];
+    __shared__ uint32_t lrow[2 * kSmallM];
+    load_exp_table(sexp, gexp);
     for (int idx = threadIdx.x; idx < m * 2 * m; idx += blockDim.x) {
         const int r = idx / (2 * m), j = idx - r * 2 * m;
         S[idx] = M[static_cast<size_t>(r) * W + j];
     }
     __syncthreads();
-    if (!cta_gauss_jordan(S, m, 2 * m, fcol, glog, gexp)) {
+    if (!cta_gauss_jordan(S, m, 2 * m, fcol, lrow, sexp, glog, gexp)) {
         if (threadIdx.x == 0)
             *status = 1;
         return;
@@ -199,16 +247,64 @@ __global__ void __launch_bounds__(kGjThreads)
              int *__restrict__ status, const uint16_t *__restrict__ glog,
              const uint16_t *__restrict__ gexp)
 {
+    extern __shared__ __align__(16) uint16_t sexp[];  // antilog table
     __shared__ uint16_t S[kPanel * 2 * kPanel];
     __shared__ uint32_t fcol[kPanel];
+    __shared__ uint32_t lrow[2 * kPanel];
     __shared__ int ksel[kPanel];
-    __shared__ int failed;
+    __shared__ int failed, fast;
     __shared__ int scan[kGjThreads];
+    // used[] as a bitmap (m <= 65535 rows)
+    __shared__ uint32_t used_bits[65536 / 32];
     const int tid = threadIdx.x, nt = blockDim.x;
-    if (tid == 0)
+    const int nwords = (m + 31) / 32;
+    if (tid == 0) {
         failed = *status != 0;
-    __syncthreads();
+        fast = 0;
+    }
+    for (int w = tid; w < nwords; w += nt) {
+        uint32_t bits = 0;
+        for (int i = 0; i < 32 && w * 32 + i < m; ++i)
+            bits |= pb.used[w * 32 + i] ? (1u << i) : 0u;
+        used_bits[w] = bits;
+    }
+    load_exp_table(sexp, gexp);
+    // Fast path: the first b unused rows as the pivot rows.  Any rows whose
+    // b x b block is invertible give the same inverse; for an invertible A
+    // this block is singular only by accident (then the search below runs).
     if (!failed) {
+        if (tid == 0) {
+            int n = 0;
+            for (int w = 0; w < nwords && n < b; ++w) {
+                uint32_t free_bits = ~used_bits[w];
+                while (free_bits && n < b) {
+                    const int r = w * 32 + __ffs(free_bits) - 1;
+                    free_bits &= free_bits - 1;
+                    if (r < m)
+                        ksel[n++] = r;
+                }
+            }
+            if (n < b)
+                failed = 1;
+        }
+        __syncthreads();
+        if (!failed) {
+            for (int idx = tid; idx < b * 2 * b; idx += nt) {
+                const int r = idx / (2 * b), j = idx - r * 2 * b;
+                S[r * 2 * kPanel + j] = j < b ? M[static_cast<size_t>(ksel[r]) * W + c0 + j]
+                                              : static_cast<uint16_t>(j - b == r);
+            }
+            __syncthreads();
+            if (cta_gauss_jordan(S, b, 2 * kPanel, fcol, lrow, sexp, glog, gexp)) {
+                for (int j = tid; j < b; j += nt)
+                    pb.used[ksel[j]] = 1;
+                if (tid == 0)
+                    fast = 1;
+            }
+            __syncthreads();
+        }
+    }
+    if (!failed && !fast) {
         // Incremental row reduction: candidate rows (unused, ascending) are
         // reduced against the pivot rows found so far (kept in reduced echelon
         // form, pivot entries 1); a candidate with a non-zero remainder
@@ -220,15 +316,6 @@ __global__ void __launch_bounds__(kGjThreads)
         __shared__ uint16_t part[kGjThreads / kPanel][kPanel];
         __shared__ int piv_col[kPanel];
         __shared__ int nk, cand, lead;
-        // used[] as a bitmap (m <= 65535 rows)
-        __shared__ uint32_t used_bits[65536 / 32];
-        const int nwords = (m + 31) / 32;
-        for (int w = tid; w < nwords; w += nt) {
-            uint32_t bits = 0;
-            for (int i = 0; i < 32 && w * 32 + i < m; ++i)
-                bits |= pb.used[w * 32 + i] ? (1u << i) : 0u;
-            used_bits[w] = bits;
-        }
         constexpr int QG = kGjThreads / kPanel;          // pivot groups summed in parallel
         const int col = tid % kPanel, qg = tid / kPanel;
         if (tid == 0) {
@@ -333,18 +420,20 @@ __global__ void __launch_bounds__(kGjThreads)
             *status = 1;
         __syncthreads();
     } else {
-        // A_KK^-1 from the current values of the pivot rows' panel columns
-        for (int idx = tid; idx < b * 2 * b; idx += nt) {
-            const int r = idx / (2 * b), j = idx - r * 2 * b;
-            S[r * 2 * kPanel + j] =
-                j < b ? M[static_cast<size_t>(ksel[r]) * W + c0 + j]
-                      : static_cast<uint16_t>(j - b == r);
-        }
-        __syncthreads();
-        if (!cta_gauss_jordan(S, b, 2 * kPanel, fcol, glog, gexp)) {
-            // cannot happen when every column found a pivot; guarded anyway
-            if (tid == 0)
-                *status = 1;
+        if (!fast) {
+            // A_KK^-1 from the current values of the pivot rows' panel columns
+            for (int idx = tid; idx < b * 2 * b; idx += nt) {
+                const int r = idx / (2 * b), j = idx - r * 2 * b;
+                S[r * 2 * kPanel + j] =
+                    j < b ? M[static_cast<size_t>(ksel[r]) * W + c0 + j]
+                          : static_cast<uint16_t>(j - b == r);
+            }
+            __syncthreads();
+            if (!cta_gauss_jordan(S, b, 2 * kPanel, fcol, lrow, sexp, glog, gexp)) {
+                // cannot happen when every column found a pivot; guarded anyway
+                if (tid == 0)
+                    *status = 1;
+            }
         }
         for (int idx = tid; idx < b * b; idx += nt) {
             const int r = idx / b, j = idx - r * b;
@@ -649,7 +738,9 @@ int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uin
     P2G_CUDA(cudaGetLastError());
     ++ctx->launches;
     if (m <= kSmallM) {
-        const size_t smem = static_cast<size_t>(m) * 2 * m * 2;
+        const size_t smem = 65536 * 2 + static_cast<size_t>(m) * 2 * m * 2;
+        P2G_CUDA(cudaFuncSetAttribute(gj_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem)));
         gj_small<<<1, kGjThreads, smem, ctx->stream>>>(M, m, W, d_inv, status, ctx->d_log,
                                                       ctx->d_exp);
         P2G_CUDA(cudaGetLastError());
@@ -673,13 +764,15 @@ int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uin
                                  ctx->stream));
         // pageable source: consumed before the call returns
     }
+    P2G_CUDA(cudaFuncSetAttribute(gj_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(kExpSmem)));
     P2G_TRY(ctx->recs2.ensure(static_cast<size_t>(kPanel) * m * 64 + kPanel * kPanel * 64));
     uint32_t *recsA = ctx->recs2.as<uint32_t>();
     uint32_t *recsO = recsA + kPanel * kPanel * 16;
     for (int c0 = 0; c0 < m; c0 += kPanel) {
         const int b = std::min(kPanel, m - c0);
-        gj_panel<<<1, kGjThreads, 0, ctx->stream>>>(M, m, W, c0, b, pb, status, ctx->d_log,
-                                                    ctx->d_exp);
+        gj_panel<<<1, kGjThreads, kExpSmem, ctx->stream>>>(M, m, W, c0, b, pb, status,
+                                                           ctx->d_log, ctx->d_exp);
         P2G_CUDA(cudaGetLastError());
         ++ctx->launches;
         P2G_TRY(records_from_matrix(ctx, pb.akk_inv, b, b, recsA));

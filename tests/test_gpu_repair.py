@@ -121,6 +121,17 @@ def test_blocked_inversion_random_and_singular(ctx):
     # the context stays usable after a singular matrix
     B = rng.integers(0, 65536, (120, 120), dtype=np.uint16)
     assert np.array_equal(ctx.invert(B), oracle.invert(B))
+    # invertible, but the leading 64 x 64 block of each panel's first unused
+    # rows is singular (rows shuffled so that pivots sit far below): the panel
+    # must fall back to searching for independent rows
+    for m in (130, 200):
+        A = rng.integers(0, 65536, (m, m), dtype=np.uint16)
+        A[:64, :64] = 0
+        A[64:128, 64:128] = 0 if m >= 128 else A[64:128, 64:128]
+        A[5, :64] = A[7, :64]          # also a rank-deficient sub-block
+        want = oracle.invert(A)
+        assert want is not None
+        assert np.array_equal(ctx.invert(A), want), m
 
 
 def test_quickpar_repair_scenarios(ctx):
