@@ -410,13 +410,15 @@ def run_verify_repair(args):
         inv_ms.append(ctx.last_timing().ms_total)
     out["invert"] = {"m": m, "ms": min(inv_ms), "method": "closed-form Vandermonde inverse "
                      "(exponents 0..m-1)"}
-    # the same inversion when the exponents are not consecutive (Gauss-Jordan)
+    # the same inversion when one recovery slice of the run is missing
     gapped = np.concatenate([np.arange(m - 1), [m + 4]]).astype(np.uint32)
     inv_ms = []
     for _ in range(2):
         ctx.reconstruction_matrix(k, dmg, gapped)
         inv_ms.append(ctx.last_timing().ms_total)
-    out["invert_gapped"] = {"m": m, "ms": min(inv_ms), "method": "blocked Gauss-Jordan"}
+    out["invert_gapped"] = {"m": m, "ms": min(inv_ms),
+                            "method": "Woodbury correction of the Vandermonde inverse "
+                                      "(one exponent outside the run)"}
     # repair
     fixed = torch.zeros((m, S), dtype=torch.uint8, device=dev)
     fbase = fixed.data_ptr()
@@ -519,8 +521,8 @@ class _GF:
 def run_invert(args):
     """The 1600 x 1600 decode matrix of the verify configuration (32000 slices):
     consecutive exponents (closed-form Vandermonde inverse) and exponents with
-    a gap (blocked Gauss-Jordan), time per call, each checked through
-    A * A^-1 = I on sampled rows."""
+    a gap (Woodbury correction of that inverse), time per call, each checked
+    through A * A^-1 = I on sampled rows."""
     import par2gpu
 
     k, m = 32000, 1600

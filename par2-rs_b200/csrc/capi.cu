@@ -385,6 +385,7 @@ int p2g_destroy(p2g_ctx *ctx)
     if (ctx->d_crc)
         cudaFree(ctx->d_crc);
     ctx->hash_out.release();
+    ctx->wb.release();
     for (p2g::DevBuf &d : ctx->spare)
         d.release();
     ctx->spare.clear();

@@ -95,6 +95,7 @@ struct p2g_ctx {
     p2g::DevBuf gj_M;      // Gauss-Jordan augmented matrix
     p2g::DevBuf gj_status; // Gauss-Jordan status + pivots
     p2g::DevBuf hash_out;  // MD5 + CRC results
+    p2g::DevBuf wb;        // decode matrices by Woodbury correction
     // Scratch buffers of destroyed batches, kept for the next batch: freeing
     // device or pinned memory synchronises the whole device, which would stall
     // a batch being prepared while another one runs.  Guarded by `mu`.

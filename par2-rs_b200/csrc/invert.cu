@@ -624,10 +624,10 @@ __global__ void vdm_quotients(const uint16_t *__restrict__ P, const uint16_t *__
     scale[j] = gexp[neg == 0 ? 0 : 65535u - neg];
 }
 
-// inv[j][r] = scale[j] * QT[e_r - s][j], through a 32 x 32 shared-memory tile
+// inv[j][r] (row stride ld) = scale[j] * QT[e_r - s][j], through a 32 x 32 shared-memory tile
 // so that both the reads (along j) and the writes (along r) are coalesced.
 __global__ void vdm_finish(const uint16_t *__restrict__ QT, const uint16_t *__restrict__ scale,
-                           const uint32_t *__restrict__ exps, uint32_t s, int m,
+                           const uint32_t *__restrict__ exps, uint32_t s, int m, int ld,
                            uint16_t *__restrict__ inv, const uint16_t *__restrict__ glog,
                            const uint16_t *__restrict__ gexp)
 {
@@ -642,7 +642,7 @@ __global__ void vdm_finish(const uint16_t *__restrict__ QT, const uint16_t *__re
     for (int jj = ty; jj < 32; jj += blockDim.y) {
         const int j = j0 + jj, r = r0 + tx;
         if (j < m && r < m)
-            inv[static_cast<size_t>(j) * m + r] =
+            inv[static_cast<size_t>(j) * ld + r] =
                 static_cast<uint16_t>(gmul(scale[j], tile[tx][jj], glog, gexp));
     }
 }
@@ -668,7 +668,7 @@ static bool exps_are_run(const uint32_t *exps, int m, uint32_t *s)
 }
 
 static int vdm_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_x, const uint32_t *d_exps,
-                      uint32_t s, uint16_t *d_inv)
+                      uint32_t s, uint16_t *d_inv, int ld)
 {
     const size_t vec = (static_cast<size_t>(m) * 2 + 255) & ~static_cast<size_t>(255);
     P2G_TRY(w.status.ensure(256 + 5 * vec));
@@ -699,13 +699,194 @@ static int vdm_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_x, const
     P2G_CUDA(cudaGetLastError());
     ++ctx->launches;
     const dim3 g2((m + 31) / 32, (m + 31) / 32), b2(32, 8);
-    vdm_finish<<<g2, b2, 0, ctx->stream>>>(QT, scale, d_exps, s, m, d_inv, ctx->d_log, ctx->d_exp);
+    vdm_finish<<<g2, b2, 0, ctx->stream>>>(QT, scale, d_exps, s, m, ld, d_inv, ctx->d_log,
+                                           ctx->d_exp);
     P2G_CUDA(cudaGetLastError());
     ++ctx->launches;
     return P2G_OK;
 }
 
 static size_t al256(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
+// ---- a few exponents outside a run: Woodbury correction --------------------
+//
+// When g of the m exponents fall outside the window [s, s+m) that holds the
+// most of them (recovery slices inside the window were lost), give each of
+// those rows one of the window's unused exponents: the result V is a permuted
+// Vandermonde matrix (closed-form inverse above) and A = V + U W differs from
+// it in g rows, U selecting the rows Q and W[q][j] = x_j^e_q + x_j^h_q.  Then
+//     A^-1 = V^-1 + V^-1 U C^-1 W V^-1,   C = I_g + W V^-1 U     (char 2: + = -)
+// costs O(g m^2): three multiply-accumulate passes and a g x g inversion.  A
+// is singular exactly when V or C is.
+
+struct WoodburyPlan {
+    uint32_t s = 0;
+    std::vector<uint32_t> vexps;    // exponents of V (a permutation of s..s+m-1)
+    std::vector<int> rows;          // Q: rows whose exponent lies outside the window
+    std::vector<uint32_t> e, h;     // their exponents in A and in V
+};
+
+// false when the exponents repeat or more than kSmallM lie outside the best window
+static bool plan_woodbury(const uint32_t *exps, int m, WoodburyPlan *wp)
+{
+    std::vector<uint32_t> sorted(exps, exps + m);
+    std::sort(sorted.begin(), sorted.end());
+    for (int i = 1; i < m; ++i)
+        if (sorted[i] == sorted[i - 1])
+            return false;
+    int best = 0, bi = 0;
+    for (int i = 0, j = 0; i < m; ++i) {
+        while (j < m && static_cast<uint64_t>(sorted[j]) < static_cast<uint64_t>(sorted[i]) + m)
+            ++j;
+        if (j - i > best) {
+            best = j - i;
+            bi = i;
+        }
+    }
+    const int g = m - best;
+    if (g == 0 || g > kSmallM)
+        return false;
+    wp->s = sorted[bi];
+    std::vector<char> taken(m, 0);
+    for (int r = 0; r < m; ++r)
+        if (exps[r] >= wp->s && exps[r] - wp->s < static_cast<uint32_t>(m))
+            taken[exps[r] - wp->s] = 1;
+    std::vector<uint32_t> holes;
+    for (int t = 0; t < m; ++t)
+        if (!taken[t])
+            holes.push_back(wp->s + t);
+    wp->vexps.assign(exps, exps + m);
+    for (int r = 0; r < m; ++r)
+        if (!(exps[r] >= wp->s && exps[r] - wp->s < static_cast<uint32_t>(m))) {
+            wp->rows.push_back(r);
+            wp->e.push_back(exps[r]);
+            wp->h.push_back(holes[wp->rows.size() - 1]);
+            wp->vexps[r] = wp->h.back();
+        }
+    return static_cast<int>(wp->rows.size()) == g && static_cast<int>(holes.size()) == g;
+}
+
+__device__ __forceinline__ uint32_t gpow(uint32_t x, uint32_t e, const uint16_t *__restrict__ glog,
+                                         const uint16_t *__restrict__ gexp)
+{
+    if (x == 0)
+        return e == 0 ? 1u : 0u;
+    return gexp[static_cast<uint32_t>((static_cast<uint64_t>(glog[x]) * e) % 65535u)];
+}
+
+// Wm[q][j] = x_j^e_q + x_j^h_q  (g x m)
+__global__ void wb_w_kernel(const uint16_t *__restrict__ x, int m, int g,
+                            const uint32_t *__restrict__ e, const uint32_t *__restrict__ h,
+                            uint16_t *__restrict__ Wm, const uint16_t *__restrict__ glog,
+                            const uint16_t *__restrict__ gexp)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, q = blockIdx.y;
+    if (j < m && q < g)
+        Wm[static_cast<size_t>(q) * m + j] =
+            static_cast<uint16_t>(gpow(x[j], e[q], glog, gexp) ^ gpow(x[j], h[q], glog, gexp));
+}
+
+// [C | I] for gj_small: C[q][q'] = [q == q'] + Y[q][rows[q']]  (row stride ldc)
+__global__ void wb_c_kernel(const uint16_t *__restrict__ Y, int ldy, const int *__restrict__ rows,
+                            int g, uint16_t *__restrict__ Caug, int ldc)
+{
+    const int q = blockIdx.x;
+    for (int c = threadIdx.x; c < 2 * g; c += blockDim.x) {
+        uint32_t v = c < g ? (Y[static_cast<size_t>(q) * ldy + rows[c]] ^ (c == q ? 1u : 0u))
+                           : (c - g == q ? 1u : 0u);
+        Caug[static_cast<size_t>(q) * ldc + c] = static_cast<uint16_t>(v);
+    }
+}
+
+// Vc[j][q] = Vinv[j][rows[q]]  (m x g)
+__global__ void wb_cols_kernel(const uint16_t *__restrict__ Vinv, int ldv, const int *__restrict__ rows,
+                               int m, int g, uint16_t *__restrict__ Vc)
+{
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx < static_cast<size_t>(m) * g) {
+        const size_t j = idx / g;
+        const int q = static_cast<int>(idx - j * g);
+        Vc[idx] = Vinv[j * ldv + rows[q]];
+    }
+}
+
+static int woodbury_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_x,
+                           const WoodburyPlan &wp, uint16_t *d_inv)
+{
+    const int g = static_cast<int>(wp.rows.size());
+    const int ld = (m + 7) & ~7;                 // u16 per row: rows 16-byte aligned
+    const int ldc = (2 * g + 7) & ~7;
+    const size_t row = static_cast<size_t>(ld) * 2;
+    // scratch: [vexps | e | h | rows | ptrs] then Vinv, Y, Z, Wm, Caug, Cinv, Vc
+    const size_t o_e = al256(m * 4), o_h = o_e + al256(g * 4), o_rows = o_h + al256(g * 4),
+                 o_ptr = o_rows + al256(g * 4), o_v = o_ptr + al256((m + 2 * g) * 8),
+                 o_y = o_v + al256(m * row), o_z = o_y + al256(g * row),
+                 o_w = o_z + al256(g * row), o_c = o_w + al256(static_cast<size_t>(g) * m * 2),
+                 o_ci = o_c + al256(static_cast<size_t>(g) * ldc * 2),
+                 o_vc = o_ci + al256(static_cast<size_t>(g) * g * 2),
+                 total = o_vc + al256(static_cast<size_t>(m) * g * 2);
+    P2G_TRY(ctx->wb.ensure(total));
+    uint8_t *b = ctx->wb.as<uint8_t>();
+    uint16_t *Vinv = reinterpret_cast<uint16_t *>(b + o_v), *Y = reinterpret_cast<uint16_t *>(b + o_y),
+             *Wm = reinterpret_cast<uint16_t *>(b + o_w),
+             *Caug = reinterpret_cast<uint16_t *>(b + o_c), *Cinv = reinterpret_cast<uint16_t *>(b + o_ci),
+             *Vc = reinterpret_cast<uint16_t *>(b + o_vc);
+    // host tables: V's exponents, e, h, rows and the row pointers of Vinv, Y, Z
+    std::vector<uint8_t> hb(o_v, 0);
+    memcpy(hb.data(), wp.vexps.data(), m * 4);
+    memcpy(hb.data() + o_e, wp.e.data(), g * 4);
+    memcpy(hb.data() + o_h, wp.h.data(), g * 4);
+    memcpy(hb.data() + o_rows, wp.rows.data(), g * 4);
+    uint8_t **ptr = reinterpret_cast<uint8_t **>(hb.data() + o_ptr);
+    for (int j = 0; j < m; ++j)
+        ptr[j] = b + o_v + j * row;
+    for (int q = 0; q < g; ++q) {
+        ptr[m + q] = b + o_y + q * row;
+        ptr[m + g + q] = b + o_z + q * row;
+    }
+    // pageable source: consumed before the call returns
+    P2G_CUDA(cudaMemcpyAsync(b, hb.data(), o_v, cudaMemcpyHostToDevice, ctx->stream));
+    uint8_t *const *pv = reinterpret_cast<uint8_t *const *>(b + o_ptr);
+    uint8_t *const *py = pv + m, *const *pz = pv + m + g;
+    const int *d_rows = reinterpret_cast<const int *>(b + o_rows);
+    // V^-1 (status cleared; set when V is singular)
+    P2G_TRY(vdm_invert(ctx, w, m, d_x, reinterpret_cast<const uint32_t *>(b), wp.s, Vinv, ld));
+    int *status = w.status.as<int>();
+    // Y = W V^-1
+    wb_w_kernel<<<dim3((m + 255) / 256, g), 256, 0, ctx->stream>>>(
+        d_x, m, g, reinterpret_cast<const uint32_t *>(b + o_e),
+        reinterpret_cast<const uint32_t *>(b + o_h), Wm, ctx->d_log, ctx->d_exp);
+    P2G_CUDA(cudaGetLastError());
+    const size_t nrec = static_cast<size_t>(m) * g * 64;
+    P2G_TRY(ctx->recs2.ensure(nrec));
+    uint32_t *recs = ctx->recs2.as<uint32_t>();
+    const size_t bytes = static_cast<size_t>(m) * 2;
+    P2G_TRY(records_from_matrix(ctx, Wm, m, g, recs));
+    P2G_TRY(muladd_run(ctx, const_cast<const uint8_t *const *>(pv), m, py, g, bytes, recs, 0));
+    // C = I + Y U, C^-1 by one CTA (status set when C is singular)
+    wb_c_kernel<<<g, 128, 0, ctx->stream>>>(Y, ld, d_rows, g, Caug, ldc);
+    P2G_CUDA(cudaGetLastError());
+    const size_t smem = 65536 * 2 + static_cast<size_t>(g) * 2 * g * 2;
+    P2G_CUDA(cudaFuncSetAttribute(gj_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem)));
+    gj_small<<<1, kGjThreads, smem, ctx->stream>>>(Caug, g, ldc, Cinv, status, ctx->d_log,
+                                                  ctx->d_exp);
+    P2G_CUDA(cudaGetLastError());
+    // Z = C^-1 Y
+    P2G_TRY(records_from_matrix(ctx, Cinv, g, g, recs));
+    P2G_TRY(muladd_run(ctx, const_cast<const uint8_t *const *>(py), g, pz, g, bytes, recs, 0));
+    // V^-1 += (V^-1 U) Z
+    const size_t nvc = static_cast<size_t>(m) * g;
+    wb_cols_kernel<<<static_cast<unsigned>((nvc + 255) / 256), 256, 0, ctx->stream>>>(Vinv, ld, d_rows,
+                                                                                   m, g, Vc);
+    P2G_CUDA(cudaGetLastError());
+    P2G_TRY(records_from_matrix(ctx, Vc, g, m, recs));
+    P2G_TRY(muladd_run(ctx, const_cast<const uint8_t *const *>(pz), g, pv, m, bytes, recs, 1));
+    P2G_CUDA(cudaMemcpy2DAsync(d_inv, bytes, Vinv, row, bytes, m, cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+    ctx->launches += 6;
+    return P2G_OK;
+}
+
 
 int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uint32_t *d_exps,
               const uint32_t *h_exps, const uint16_t *d_A, uint16_t *d_inv)
@@ -714,7 +895,10 @@ int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uin
         return P2G_OK;
     uint32_t s = 0;
     if (!d_A && h_exps && exps_are_run(h_exps, m, &s))
-        return vdm_invert(ctx, w, m, d_cmiss, d_exps, s, d_inv);
+        return vdm_invert(ctx, w, m, d_cmiss, d_exps, s, d_inv, m);
+    WoodburyPlan wp;
+    if (!d_A && h_exps && m > kSmallM && plan_woodbury(h_exps, m, &wp))
+        return woodbury_invert(ctx, w, m, d_cmiss, wp, d_inv);
     const int W = (2 * m + 7) & ~7;  // row stride in u16: rows are 16-byte aligned
     const size_t row_bytes = static_cast<size_t>(W) * 2;
     P2G_TRY(w.M.ensure(static_cast<size_t>(m) * row_bytes));

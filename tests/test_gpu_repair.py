@@ -26,17 +26,25 @@ def par2_matrix(k, missing, exps):
 
 def exponent_set(kind, m, rng):
     """run: 0..m-1 and offset/perm: a permuted run s..s+m-1 (closed-form
-    Vandermonde inverse); gapped: not consecutive (Gauss-Jordan)."""
+    Vandermonde inverse); gapped / gaps / far / below: a few exponents outside
+    the best window (Woodbury correction above 96, Gauss-Jordan below)."""
     if kind == "run":
         return np.arange(m)
     if kind == "offset":
         return np.arange(7, 7 + m)
     if kind == "perm":
         return rng.permutation(np.arange(3, 3 + m))
-    return np.concatenate([np.arange(m - 1), [m + 4]])
+    if kind == "gapped":
+        return np.concatenate([np.arange(m - 1), [m + 4]])
+    if kind == "gaps":       # lost recovery slices 2, 5, 9, 10 of the lowest m + 4
+        keep = [e for e in range(m + 4) if e not in (2, 5, 9, 10)][:m]
+        return rng.permutation(np.array(keep))
+    if kind == "far":
+        return np.array(([60000, 40001, 65534] + list(range(1, m)))[:m])
+    return np.array(([0, 1] + list(range(50, 50 + m)))[:m])   # two below the window
 
 
-@pytest.mark.parametrize("kind", ["run", "offset", "perm", "gapped"])
+@pytest.mark.parametrize("kind", ["run", "offset", "perm", "gapped", "gaps", "far", "below"])
 @pytest.mark.parametrize("m", [1, 2, 13, 64, 96, 97, 130, 200, 333])
 def test_reconstruction_matrix_matches_oracle(ctx, m, kind):
     rng = np.random.default_rng(m)
@@ -58,7 +66,7 @@ def test_reconstruction_matrix_large_run(ctx):
                           oracle.invert(par2_matrix(k, missing, exps)))
 
 
-@pytest.mark.parametrize("kind", ["run", "gapped"])
+@pytest.mark.parametrize("kind", ["run", "gapped", "woodbury"])
 def test_repeated_constants_are_singular(ctx, kind):
     """Beyond 32768 slices the PAR2 constants repeat (c_i = c_{i+32768}):
     losing both slices of such a pair is unrepairable on either path."""
@@ -69,6 +77,9 @@ def test_repeated_constants_are_singular(ctx, kind):
     assert c[5] == c[5 + 32768]
     missing = np.array([5, 9, 5 + 32768])
     exps = np.arange(3) if kind == "run" else np.array([0, 1, 3])
+    if kind == "woodbury":   # m = 150 with one exponent outside the window
+        missing = np.sort(np.concatenate([[5, 5 + 32768], np.arange(100, 248)]))
+        exps = np.concatenate([np.arange(149), [200]])
     with pytest.raises(par2gpu.Par2GpuError) as ei:
         ctx.reconstruction_matrix(k, missing, exps)
     assert ei.value.code == par2gpu.ESINGULAR
