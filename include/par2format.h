@@ -1,0 +1,53 @@
+/* par2format.h -- create and repair of PAR2 sets from files on one GPU.
+ *
+ * The top-level operations of par2-rs over the GPU codec (libpar2gpu):
+ *   p2f_create  Par2Creator::new(..).with_*(..).create()   creator.rs:148-521
+ *   p2f_repair  Par2Repairer::repair                       lib.rs:132-351
+ * Files are written with par2-rs's packets, packet order, volume names and
+ * creator text.  Every call returns P2F_OK (0) or a negative code; the
+ * message of the last failure on this thread is p2f_last_error().
+ * Built as par2-rs_b200/lib/libpar2format.so (needs libpar2gpu.so). */
+#ifndef PAR2FORMAT_H
+#define PAR2FORMAT_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define P2F_OK 0
+#define P2F_ERROR (-1)          /* Par2Error::InvalidFormat / Io: see p2f_last_error */
+#define P2F_ESINGULAR (-4)      /* Par2Error::RepairFailed("Singular matrix") */
+#define P2F_EINSUFFICIENT (-8)  /* Par2Error::InsufficientRecovery (error.rs:5-39) */
+
+#define P2F_SCHEME_SINGLE 0       /* VolumeScheme::Single (volumes.rs:27-31) */
+#define P2F_SCHEME_EXPONENTIAL 1  /* VolumeScheme::Exponential: 1, 2, 4 ... slices per file */
+
+/* Phase times of one call (milliseconds) and what it processed. */
+typedef struct p2f_stats {
+    double ms_scan, ms_ingest, ms_gpu, ms_write, ms_total;
+    uint64_t block_size, data_blocks, recovery_blocks, bytes_read;
+    uint64_t damaged_blocks, files_written;
+} p2f_stats;
+
+/* Creates the set of `inputs` (n paths) at `output` (the index .par2; NULL:
+ * the first input with its extensions replaced by .par2, creator.rs:170).
+ * block_size 0 picks it as par2-rs does (creator.rs:30-67); otherwise it
+ * must be a multiple of 4 and at least 2048.  The paths of the written files
+ * are not returned: they follow volumes.rs:65-78.  stats may be NULL. */
+int p2f_create(const char *const *inputs, size_t n, const char *output, uint64_t block_size,
+               float redundancy_percent, int scheme, p2f_stats *stats);
+
+/* Verifies the files of the set `par2_path` (with its volumes, found by
+ * recovery set ID) in directory `dir` and rebuilds damaged or missing slices
+ * in place.  *rebuilt (may be NULL) receives the number of slices rebuilt,
+ * 0 when every slice was intact. */
+int p2f_repair(const char *par2_path, const char *dir, uint64_t *rebuilt, p2f_stats *stats);
+
+const char *p2f_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,93 @@
+// format_capi.cpp -- the C ABI of par2format.h over par2_pipeline.hpp.
+#include "../../include/par2format.h"
+
+#include <string>
+
+#include "par2_pipeline.hpp"
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(const std::exception &e)
+{
+    g_error = e.what();
+    if (g_error.find("Singular matrix") != std::string::npos)
+        return P2F_ESINGULAR;
+    if (g_error.find("Insufficient recovery") != std::string::npos)
+        return P2F_EINSUFFICIENT;
+    return P2F_ERROR;
+}
+
+void fill(p2f_stats *out, const par2::PipelineStats &s)
+{
+    if (!out)
+        return;
+    out->ms_scan = s.ms_scan;
+    out->ms_ingest = s.ms_ingest;
+    out->ms_gpu = s.ms_gpu;
+    out->ms_write = s.ms_write;
+    out->ms_total = s.ms_total;
+    out->block_size = s.block_size;
+    out->data_blocks = s.data_blocks;
+    out->recovery_blocks = s.recovery_blocks;
+    out->bytes_read = s.bytes_read;
+    out->damaged_blocks = s.damaged_blocks;
+    out->files_written = s.files_written;
+}
+
+}  // namespace
+
+extern "C" {
+
+int p2f_create(const char *const *inputs, size_t n, const char *output, uint64_t block_size,
+               float redundancy_percent, int scheme, p2f_stats *stats)
+{
+    g_error.clear();
+    try {
+        if (!inputs && n)
+            throw par2::Par2Error("p2f_create: null input list");
+        std::vector<std::filesystem::path> in;
+        for (size_t i = 0; i < n; ++i) {
+            if (!inputs[i])
+                throw par2::Par2Error("p2f_create: null input path");
+            in.emplace_back(inputs[i]);
+        }
+        if (scheme != P2F_SCHEME_SINGLE && scheme != P2F_SCHEME_EXPONENTIAL)
+            throw par2::Par2Error("p2f_create: unknown volume scheme");
+        par2::Par2Creator c(in);
+        c.with_redundancy(redundancy_percent)
+            .with_volume_scheme(scheme == P2F_SCHEME_SINGLE ? par2::VolumeScheme::Single
+                                                            : par2::VolumeScheme::Exponential);
+        if (output)
+            c.with_output_path(output);
+        if (block_size)
+            c.with_block_size(block_size);
+        c.create();
+        fill(stats, c.stats());
+        return P2F_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+int p2f_repair(const char *par2_path, const char *dir, uint64_t *rebuilt, p2f_stats *stats)
+{
+    g_error.clear();
+    try {
+        if (!par2_path || !dir)
+            throw par2::Par2Error("p2f_repair: null path");
+        par2::Par2Repairer r(par2_path, dir);
+        const uint64_t n = r.repair();
+        if (rebuilt)
+            *rebuilt = n;
+        fill(stats, r.stats());
+        return P2F_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+const char *p2f_last_error(void) { return g_error.c_str(); }
+
+}  // extern "C"

@@ -1,17 +1,14 @@
 // par2_format.hpp -- the PAR2 on-disk format around the GPU codec: packet
-// writing and parsing, volume naming and the create pipeline, with the
-// behaviour of par2-rs:
+// writing and parsing, volume naming and block counts, with the behaviour of
+// par2-rs:
 //
 //   packet layout, bodies, File ID, set ID     writer.rs:23-264
 //   File ID order (little-endian compare)      parser.rs:556-565
 //   scan / parse / volume discovery / order    parser.rs:181-547, 566-800
 //   volume split and file names                volumes.rs:27-210
 //   block size, block and recovery counts      creator.rs:30-67, 261-352
-//   file layout of every written .par2         creator.rs:453-521
 //
-// The IFSC checksums (MD5 + CRC32 of every zero-padded slice) and the
-// recovery slices of Par2Creator::create come from the GPU (p2g_hash_slices,
-// p2g_encode); the host computes only the per-file MD5s and packet hashes.
+// The create and repair pipelines over it are in par2_pipeline.hpp.
 #pragma once
 #include <stdint.h>
 #include <stdio.h>
@@ -603,202 +600,6 @@ class Par2File {
                              return ra != rb ? ra < rb : file_id_less(a.file_id, b.file_id);
                          });
     }
-};
-
-// ---- creator (creator.rs) ---------------------------------------------------
-
-class Par2Creator {
-  public:
-    explicit Par2Creator(std::vector<std::filesystem::path> input_files)
-        : inputs_(std::move(input_files))
-    {
-        if (inputs_.empty())
-            throw Par2Error("No input files");
-        for (const auto &f : inputs_)
-            if (!std::filesystem::exists(f))
-                throw Par2Error("Input file does not exist: " + f.string());
-        // first input with its extensions replaced: a.b.c -> a.par2 (creator.rs:170)
-        output_ = inputs_[0];
-        output_.replace_extension("");
-        output_.replace_extension("par2");
-    }
-    Par2Creator &with_block_size(uint64_t size)
-    {
-        if (size == 0)
-            throw Par2Error("Block size cannot be zero");
-        if (size < 2048)
-            throw Par2Error("Block size must be at least 2048 bytes (got " + std::to_string(size) + ")");
-        if (size % 4)
-            throw Par2Error("Block size must be multiple of 4");
-        block_size_ = size;
-        return *this;
-    }
-    Par2Creator &with_redundancy(float percent)
-    {
-        if (percent != percent || percent - percent != 0)
-            throw Par2Error("Redundancy percentage must be a finite number");
-        if (percent < 0)
-            throw Par2Error("Redundancy percentage cannot be negative");
-        percent_ = percent;
-        return *this;
-    }
-    Par2Creator &with_output_path(std::filesystem::path p)
-    {
-        output_ = std::move(p);
-        return *this;
-    }
-    Par2Creator &with_volume_scheme(VolumeScheme s)
-    {
-        scheme_ = s;
-        return *this;
-    }
-    Par2Creator &with_creator_text(std::string t)
-    {
-        creator_ = std::move(t);
-        return *this;
-    }
-
-    // Writes the index file and the volumes; returns their paths.
-    std::vector<std::filesystem::path> create() const
-    {
-        // per-file MD5s and File IDs, files in File ID order
-        std::vector<FileInfo> infos;
-        std::vector<std::filesystem::path> paths;
-        for (const auto &in : inputs_) {
-            FileInfo fi;
-            fi.name = in.filename().string();
-            std::vector<uint8_t> data = read_all(in);
-            fi.length = data.size();
-            fi.hash = Md5::of(data.data(), data.size());
-            fi.hash_16k = Md5::of(data.data(), std::min<size_t>(data.size(), 16384));
-            fi.file_id = compute_file_id(fi.hash_16k, fi.length, fi.name);
-            infos.push_back(fi);
-            paths.push_back(in);
-        }
-        std::vector<size_t> order(infos.size());
-        for (size_t i = 0; i < order.size(); ++i)
-            order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-            return file_id_less(infos[a].file_id, infos[b].file_id);
-        });
-        uint64_t total = 0;
-        for (const FileInfo &f : infos)
-            total += f.length;
-        const uint64_t bs = block_size_ ? block_size_ : calculate_block_size(total);
-        std::vector<size_t> nblk(infos.size());
-        uint64_t k = 0;
-        for (size_t i : order) {
-            nblk[i] = static_cast<size_t>((infos[i].length + bs - 1) / bs);
-            k += nblk[i];
-        }
-        if (k > 65535)
-            throw Par2Error("Total data blocks (" + std::to_string(k) +
-                            ") exceed GF(2^16) limit (65535)");
-        const uint64_t r = recovery_block_count(k, bs, percent_);
-        if (r > 65535)
-            throw Par2Error("Recovery blocks (" + std::to_string(r) + ") exceed GF(2^16) limit (65535)");
-        if (k + r > 65535)
-            throw Par2Error("Total blocks (data + recovery) exceed GF(2^16) limit (65535)");
-        // the slices, zero-padded, in canonical order
-        std::vector<uint8_t> slices(static_cast<size_t>(k * bs), 0);
-        size_t g = 0;
-        for (size_t i : order) {
-            std::vector<uint8_t> data = read_all(paths[i]);
-            memcpy(slices.data() + g * bs, data.data(), data.size());
-            g += nblk[i];
-        }
-        std::vector<const uint8_t *> sp(k);
-        for (uint64_t i = 0; i < k; ++i)
-            sp[i] = slices.data() + i * bs;
-        // IFSC checksums and recovery slices on the GPU
-        std::vector<uint8_t> md5(k * 16);
-        std::vector<uint32_t> crc(k);
-        if (k)
-            check(p2g_hash_slices(codec_ctx(), sp.data(), k, bs, md5.data(), crc.data(), 0));
-        std::vector<uint8_t> rec(static_cast<size_t>(r * bs));
-        std::vector<uint8_t *> rp(r);
-        std::vector<uint32_t> exps(r);
-        for (uint64_t e = 0; e < r; ++e) {
-            rp[e] = rec.data() + e * bs;
-            exps[e] = static_cast<uint32_t>(e);
-        }
-        if (k && r)
-            check(p2g_encode(codec_ctx(), sp.data(), k, bs, exps.data(), r, rp.data(), 0));
-        // packets shared by every file
-        std::vector<FileHash> ids;
-        for (size_t i : order)
-            ids.push_back(infos[i].file_id);
-        const FileHash set_id = compute_recovery_set_id(build_main_packet_body(bs, ids));
-        std::vector<uint8_t> common;
-        write_packet(common, packet_types::CREATOR, set_id,
-                     std::vector<uint8_t>(creator_.begin(), creator_.end()));
-        write_packet(common, packet_types::MAIN, set_id, build_main_packet_body(bs, ids));
-        for (size_t i : order)
-            write_packet(common, packet_types::FILE_DESC, set_id, file_desc_body(infos[i]));
-        g = 0;
-        for (size_t i : order) {
-            std::vector<SliceChecksum> cs(nblk[i]);
-            for (size_t b = 0; b < nblk[i]; ++b, ++g) {
-                memcpy(cs[b].md5.data(), md5.data() + g * 16, 16);
-                cs[b].crc32 = crc[g];
-            }
-            write_packet(common, packet_types::IFSC, set_id, ifsc_body(infos[i].file_id, cs));
-        }
-        // files: Single = everything in the index file; otherwise an index
-        // file without recovery slices plus the volumes (creator.rs:441-521)
-        std::vector<uint32_t> all(r);
-        for (uint64_t e = 0; e < r; ++e)
-            all[e] = static_cast<uint32_t>(e);
-        std::vector<VolumeInfo> vols = split_into_volumes(all, scheme_, output_);
-        if (scheme_ == VolumeScheme::Single && !vols.empty()) {
-            vols[0].path = output_;
-        } else {
-            VolumeInfo index;
-            index.path = output_;
-            vols.insert(vols.begin(), index);
-        }
-        std::vector<std::filesystem::path> written;
-        for (const VolumeInfo &v : vols) {
-            std::vector<uint8_t> out = common;
-            for (uint32_t e : v.exponents)
-                write_packet(out, packet_types::RECV_SLICE, set_id,
-                             recovery_body(e, rec.data() + static_cast<size_t>(e) * bs, bs));
-            write_all(v.path, out);
-            written.push_back(v.path);
-        }
-        return written;
-    }
-
-  private:
-    static std::vector<uint8_t> read_all(const std::filesystem::path &p)
-    {
-        FILE *f = fopen(p.string().c_str(), "rb");
-        if (!f)
-            throw Par2Error("Failed to open " + p.string());
-        std::vector<uint8_t> d(static_cast<size_t>(std::filesystem::file_size(p)));
-        const size_t got = d.empty() ? 0 : fread(d.data(), 1, d.size(), f);
-        fclose(f);
-        if (got != d.size())
-            throw Par2Error("Failed to read " + p.string());
-        return d;
-    }
-    static void write_all(const std::filesystem::path &p, const std::vector<uint8_t> &d)
-    {
-        FILE *f = fopen(p.string().c_str(), "wb");
-        if (!f || fwrite(d.data(), 1, d.size(), f) != d.size()) {
-            if (f)
-                fclose(f);
-            throw Par2Error("Failed to write " + p.string());
-        }
-        fclose(f);
-    }
-
-    std::vector<std::filesystem::path> inputs_;
-    std::filesystem::path output_;
-    uint64_t block_size_ = 0;
-    float percent_ = 5.0f;
-    VolumeScheme scheme_ = VolumeScheme::Exponential;
-    std::string creator_ = kReferenceCreator;
 };
 
 }  // namespace par2

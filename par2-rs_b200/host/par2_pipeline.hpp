@@ -1,0 +1,523 @@
+// par2_pipeline.hpp -- create and repair of PAR2 sets from files, with the
+// slices resident on the GPU:
+//
+//   Par2Creator::create      creator.rs:261-521  (new, with_* options 148-253)
+//   Par2Repairer::repair     lib.rs:132-351, repair.rs:537-604 (verify, lowest
+//                            exponents, rebuild, write back)
+//
+// Files stream through pinned host buffers straight into one device buffer of
+// zero-padded slices: a pool of reader threads each reads a file in 8 MiB
+// chunks, folds every chunk into the file's MD5 on the host (whole-file MD5 is
+// a serial chain) and uploads it on its own stream while reading the next
+// chunk.  The IFSC checksums, the slice verification and the recovery slices
+// are computed from that buffer by libpar2gpu (P2G_DEVICE_PTRS); only the
+// recovery slices come back to the host.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <set>
+#include <thread>
+
+#include "par2_format.hpp"
+
+namespace par2 {
+
+struct PipelineStats {
+    double ms_scan = 0;    // sizes, first-16-KiB MD5s, File IDs, order
+    double ms_ingest = 0;  // read + whole-file MD5 + upload of every file
+    double ms_gpu = 0;     // IFSC / verification + encode / repair on the device
+    double ms_write = 0;   // packets and files (create) / repaired files (repair)
+    double ms_total = 0;
+    uint64_t block_size = 0, data_blocks = 0, recovery_blocks = 0, bytes_read = 0;
+    uint64_t damaged_blocks = 0, files_written = 0;
+};
+
+namespace detail {
+
+inline double ms_since(std::chrono::steady_clock::time_point t0)
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+inline void cuda_check(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw Par2Error(std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+// Device buffer of k zero-padded slices of bs bytes.
+class DeviceSlices {
+  public:
+    DeviceSlices(uint64_t k, uint64_t bs) : k_(k), bs_(bs)
+    {
+        if (k && bs) {
+            cuda_check(cudaMalloc(&p_, k * bs), "cudaMalloc (slices)");
+            cuda_check(cudaMemset(p_, 0, k * bs), "cudaMemset (slices)");
+        }
+    }
+    ~DeviceSlices()
+    {
+        if (p_)
+            cudaFree(p_);
+    }
+    DeviceSlices(const DeviceSlices &) = delete;
+    DeviceSlices &operator=(const DeviceSlices &) = delete;
+    uint8_t *slice(uint64_t i) const { return static_cast<uint8_t *>(p_) + i * bs_; }
+    std::vector<const uint8_t *> ptrs(uint64_t first, uint64_t n) const
+    {
+        std::vector<const uint8_t *> v(n);
+        for (uint64_t i = 0; i < n; ++i)
+            v[i] = slice(first + i);
+        return v;
+    }
+
+  private:
+    void *p_ = nullptr;
+    uint64_t k_, bs_;
+};
+
+struct IngestJob {
+    std::filesystem::path path;
+    uint8_t *dst = nullptr;   // device: the file's first slice
+    uint64_t length = 0;      // bytes to read (file length)
+    FileHash md5{};           // out: MD5 of what was read
+    bool ok = false;          // out: the file existed and had `length` bytes
+};
+
+// Reads every job's file into device memory with whole-file MD5s, `threads`
+// files at a time.
+inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads)
+{
+    constexpr size_t kChunk = 8u << 20;
+    std::atomic<size_t> next{0};
+    std::atomic<uint64_t> total{0};
+    std::vector<std::string> errors(threads);
+    auto worker = [&](unsigned t) {
+        cudaStream_t st = nullptr;
+        uint8_t *buf[2] = {nullptr, nullptr};
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        try {
+            cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+            for (int b = 0; b < 2; ++b) {
+                cuda_check(cudaMallocHost(reinterpret_cast<void **>(&buf[b]), kChunk), "cudaMallocHost");
+                cuda_check(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming), "cudaEventCreate");
+            }
+            for (size_t j; (j = next.fetch_add(1)) < jobs.size();) {
+                IngestJob &job = jobs[j];
+                FILE *f = fopen(job.path.string().c_str(), "rb");
+                if (!f)
+                    continue;  // missing file: its slices stay zero
+                Md5 h;
+                uint64_t off = 0;
+                int b = 0;
+                while (off < job.length) {
+                    cuda_check(cudaEventSynchronize(ev[b]), "cudaEventSynchronize");
+                    const size_t n = fread(buf[b], 1, std::min<uint64_t>(kChunk, job.length - off), f);
+                    if (n == 0)
+                        break;
+                    h.update(buf[b], n);
+                    cuda_check(cudaMemcpyAsync(job.dst + off, buf[b], n, cudaMemcpyHostToDevice, st),
+                               "cudaMemcpyAsync");
+                    cuda_check(cudaEventRecord(ev[b], st), "cudaEventRecord");
+                    off += n;
+                    b ^= 1;
+                }
+                uint8_t extra;
+                job.ok = off == job.length && fread(&extra, 1, 1, f) == 0;
+                fclose(f);
+                job.md5 = h.finalize();
+                total += off;
+            }
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        } catch (const std::exception &e) {
+            errors[t] = e.what();
+        }
+        for (int b = 0; b < 2; ++b) {
+            if (ev[b])
+                cudaEventDestroy(ev[b]);
+            if (buf[b])
+                cudaFreeHost(buf[b]);
+        }
+        if (st)
+            cudaStreamDestroy(st);
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < threads; ++t)
+        pool.emplace_back(worker, t);
+    for (auto &th : pool)
+        th.join();
+    for (const std::string &e : errors)
+        if (!e.empty())
+            throw Par2Error(e);
+    return total;
+}
+
+inline unsigned reader_threads(size_t files)
+{
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    return static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(files, hw)));
+}
+
+inline std::vector<uint8_t> read_head(const std::filesystem::path &p, size_t n)
+{
+    std::vector<uint8_t> d(n);
+    FILE *f = fopen(p.string().c_str(), "rb");
+    if (!f)
+        throw Par2Error("Failed to open " + p.string());
+    const size_t got = n ? fread(d.data(), 1, n, f) : 0;
+    fclose(f);
+    d.resize(got);
+    return d;
+}
+
+inline void write_file(const std::filesystem::path &p, const uint8_t *d, size_t n)
+{
+    FILE *f = fopen(p.string().c_str(), "wb");
+    if (!f || (n && fwrite(d, 1, n, f) != n)) {
+        if (f)
+            fclose(f);
+        throw Par2Error("Failed to write " + p.string());
+    }
+    fclose(f);
+}
+
+}  // namespace detail
+
+class Par2Creator {
+  public:
+    explicit Par2Creator(std::vector<std::filesystem::path> input_files)
+        : inputs_(std::move(input_files))
+    {
+        if (inputs_.empty())
+            throw Par2Error("No input files");
+        for (const auto &f : inputs_)
+            if (!std::filesystem::exists(f))
+                throw Par2Error("Input file does not exist: " + f.string());
+        // first input with its extensions replaced: a.b.c -> a.par2 (creator.rs:170)
+        output_ = inputs_[0];
+        output_.replace_extension("");
+        output_.replace_extension("par2");
+    }
+    Par2Creator &with_block_size(uint64_t size)
+    {
+        if (size == 0)
+            throw Par2Error("Block size cannot be zero");
+        if (size < 2048)
+            throw Par2Error("Block size must be at least 2048 bytes (got " + std::to_string(size) + ")");
+        if (size % 4)
+            throw Par2Error("Block size must be multiple of 4");
+        block_size_ = size;
+        return *this;
+    }
+    Par2Creator &with_redundancy(float percent)
+    {
+        if (percent != percent || percent - percent != 0)
+            throw Par2Error("Redundancy percentage must be a finite number");
+        if (percent < 0)
+            throw Par2Error("Redundancy percentage cannot be negative");
+        percent_ = percent;
+        return *this;
+    }
+    Par2Creator &with_output_path(std::filesystem::path p)
+    {
+        output_ = std::move(p);
+        return *this;
+    }
+    Par2Creator &with_volume_scheme(VolumeScheme s)
+    {
+        scheme_ = s;
+        return *this;
+    }
+    Par2Creator &with_creator_text(std::string t)
+    {
+        creator_ = std::move(t);
+        return *this;
+    }
+    const PipelineStats &stats() const { return stats_; }
+
+    // Writes the index file and the volumes; returns their paths.
+    std::vector<std::filesystem::path> create()
+    {
+        using detail::ms_since;
+        const auto t0 = std::chrono::steady_clock::now();
+        stats_ = PipelineStats();
+        // File IDs need only the first 16 KiB; the order fixes the slice layout
+        std::vector<FileInfo> infos(inputs_.size());
+        for (size_t i = 0; i < inputs_.size(); ++i) {
+            FileInfo &fi = infos[i];
+            fi.name = inputs_[i].filename().string();
+            fi.length = std::filesystem::file_size(inputs_[i]);
+            const std::vector<uint8_t> head = detail::read_head(inputs_[i], 16384);
+            fi.hash_16k = Md5::of(head.data(), head.size());
+            fi.file_id = compute_file_id(fi.hash_16k, fi.length, fi.name);
+        }
+        std::vector<size_t> order(infos.size());
+        for (size_t i = 0; i < order.size(); ++i)
+            order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+            return file_id_less(infos[a].file_id, infos[b].file_id);
+        });
+        uint64_t total = 0;
+        for (const FileInfo &f : infos)
+            total += f.length;
+        const uint64_t bs = block_size_ ? block_size_ : calculate_block_size(total);
+        std::vector<uint64_t> first(infos.size()), nblk(infos.size());
+        uint64_t k = 0;
+        for (size_t i : order) {
+            first[i] = k;
+            nblk[i] = (infos[i].length + bs - 1) / bs;
+            k += nblk[i];
+        }
+        if (k > 65535)
+            throw Par2Error("Total data blocks (" + std::to_string(k) + ") exceed GF(2^16) limit (65535)");
+        const uint64_t r = recovery_block_count(k, bs, percent_);
+        if (r > 65535)
+            throw Par2Error("Recovery blocks (" + std::to_string(r) + ") exceed GF(2^16) limit (65535)");
+        if (k + r > 65535)
+            throw Par2Error("Total blocks (data + recovery) exceed GF(2^16) limit (65535)");
+        stats_.block_size = bs;
+        stats_.data_blocks = k;
+        stats_.recovery_blocks = r;
+        stats_.ms_scan = ms_since(t0);
+        // every file once: whole-file MD5 on the host, slices to the device
+        const auto t1 = std::chrono::steady_clock::now();
+        codec_ctx();  // the device context exists before the readers start
+        detail::DeviceSlices dev(k, bs);
+        std::vector<detail::IngestJob> jobs(infos.size());
+        for (size_t i = 0; i < infos.size(); ++i) {
+            jobs[i].path = inputs_[i];
+            jobs[i].dst = k ? dev.slice(first[i]) : nullptr;
+            jobs[i].length = infos[i].length;
+        }
+        stats_.bytes_read = detail::ingest(jobs, detail::reader_threads(jobs.size()));
+        for (size_t i = 0; i < infos.size(); ++i) {
+            if (!jobs[i].ok)
+                throw Par2Error("Failed to read " + inputs_[i].string());
+            infos[i].hash = jobs[i].md5;
+        }
+        stats_.ms_ingest = ms_since(t1);
+        // IFSC checksums and recovery slices from the device-resident slices
+        const auto t2 = std::chrono::steady_clock::now();
+        std::vector<uint8_t> md5(k * 16), rec(static_cast<size_t>(r * bs));
+        std::vector<uint32_t> crc(k);
+        if (k) {
+            std::vector<const uint8_t *> sp = dev.ptrs(0, k);
+            check(p2g_hash_slices(codec_ctx(), sp.data(), k, bs, md5.data(), crc.data(),
+                                  P2G_DEVICE_PTRS));
+            if (r) {
+                detail::DeviceSlices out(r, bs);
+                std::vector<uint8_t *> op(r);
+                std::vector<uint32_t> exps(r);
+                for (uint64_t e = 0; e < r; ++e) {
+                    op[e] = out.slice(e);
+                    exps[e] = static_cast<uint32_t>(e);
+                }
+                check(p2g_encode(codec_ctx(), sp.data(), k, bs, exps.data(), r, op.data(),
+                                 P2G_DEVICE_PTRS));
+                detail::cuda_check(cudaMemcpy(rec.data(), out.slice(0), r * bs, cudaMemcpyDeviceToHost),
+                                   "cudaMemcpy (recovery slices)");
+            }
+        }
+        stats_.ms_gpu = ms_since(t2);
+        // packets shared by every file, then one file per volume (creator.rs:441-521)
+        const auto t3 = std::chrono::steady_clock::now();
+        std::vector<FileHash> ids;
+        for (size_t i : order)
+            ids.push_back(infos[i].file_id);
+        const FileHash set_id = compute_recovery_set_id(build_main_packet_body(bs, ids));
+        std::vector<uint8_t> common;
+        write_packet(common, packet_types::CREATOR, set_id,
+                     std::vector<uint8_t>(creator_.begin(), creator_.end()));
+        write_packet(common, packet_types::MAIN, set_id, build_main_packet_body(bs, ids));
+        for (size_t i : order)
+            write_packet(common, packet_types::FILE_DESC, set_id, file_desc_body(infos[i]));
+        for (size_t i : order) {
+            std::vector<SliceChecksum> cs(nblk[i]);
+            for (uint64_t b = 0; b < nblk[i]; ++b) {
+                memcpy(cs[b].md5.data(), md5.data() + (first[i] + b) * 16, 16);
+                cs[b].crc32 = crc[first[i] + b];
+            }
+            write_packet(common, packet_types::IFSC, set_id, ifsc_body(infos[i].file_id, cs));
+        }
+        std::vector<uint32_t> all(r);
+        for (uint64_t e = 0; e < r; ++e)
+            all[e] = static_cast<uint32_t>(e);
+        std::vector<VolumeInfo> vols = split_into_volumes(all, scheme_, output_);
+        if (scheme_ == VolumeScheme::Single && !vols.empty()) {
+            vols[0].path = output_;
+        } else {
+            VolumeInfo index;
+            index.path = output_;
+            vols.insert(vols.begin(), index);
+        }
+        std::vector<std::filesystem::path> written;
+        for (const VolumeInfo &v : vols) {
+            std::vector<uint8_t> out = common;
+            for (uint32_t e : v.exponents)
+                write_packet(out, packet_types::RECV_SLICE, set_id,
+                             recovery_body(e, rec.data() + static_cast<size_t>(e) * bs, bs));
+            detail::write_file(v.path, out.data(), out.size());
+            written.push_back(v.path);
+        }
+        stats_.files_written = written.size();
+        stats_.ms_write = ms_since(t3);
+        stats_.ms_total = ms_since(t0);
+        return written;
+    }
+
+  private:
+    std::vector<std::filesystem::path> inputs_;
+    std::filesystem::path output_;
+    uint64_t block_size_ = 0;
+    float percent_ = 5.0f;
+    VolumeScheme scheme_ = VolumeScheme::Exponential;
+    std::string creator_ = kReferenceCreator;
+    PipelineStats stats_;
+};
+
+// Verification and repair of the files of a set in `dir`: every slice is
+// checked against its IFSC entry on the GPU (a missing or short file counts
+// as damaged where it lacks data), the damaged slices are rebuilt from the m
+// lowest recovery exponents (repair.rs:537-604) and the touched files are
+// rewritten; finally every rewritten file's MD5 is checked against its
+// FileDesc entry.
+class Par2Repairer {
+  public:
+    Par2Repairer(std::filesystem::path par2, std::filesystem::path dir)
+        : par2_(std::move(par2)), dir_(std::move(dir))
+    {
+    }
+    const PipelineStats &stats() const { return stats_; }
+
+    // returns the number of slices rebuilt (0: nothing was damaged)
+    uint64_t repair()
+    {
+        using detail::ms_since;
+        const auto t0 = std::chrono::steady_clock::now();
+        stats_ = PipelineStats();
+        Par2File p = Par2File::load(par2_);
+        const uint64_t bs = p.block_size;
+        std::vector<uint64_t> first, nblk;
+        uint64_t k = 0;
+        for (const FileInfo &f : p.files_in_order) {
+            first.push_back(k);
+            nblk.push_back((f.length + bs - 1) / bs);
+            k += nblk.back();
+        }
+        if (k > 65535)
+            throw Par2Error("Total data blocks exceed GF(2^16) limit (65535)");
+        stats_.block_size = bs;
+        stats_.data_blocks = k;
+        stats_.recovery_blocks = p.recovery_blocks.size();
+        stats_.ms_scan = ms_since(t0);
+        const auto t1 = std::chrono::steady_clock::now();
+        codec_ctx();
+        detail::DeviceSlices dev(k, bs);
+        std::vector<detail::IngestJob> jobs(p.files_in_order.size());
+        for (size_t i = 0; i < jobs.size(); ++i) {
+            jobs[i].path = dir_ / p.files_in_order[i].name;
+            jobs[i].dst = k ? dev.slice(first[i]) : nullptr;
+            jobs[i].length = p.files_in_order[i].length;
+        }
+        stats_.bytes_read = detail::ingest(jobs, detail::reader_threads(jobs.size()));
+        stats_.ms_ingest = ms_since(t1);
+        const auto t2 = std::chrono::steady_clock::now();
+        // per-slice verification on the device
+        std::vector<uint64_t> damaged;
+        if (k) {
+            std::vector<uint8_t> md5(k * 16, 0), ok(k, 0);
+            std::vector<uint32_t> crc(k, 0);
+            std::vector<bool> listed(k, false);
+            for (size_t i = 0; i < p.files_in_order.size(); ++i) {
+                const auto it = p.slice_checksums.find(p.files_in_order[i].file_id);
+                if (it == p.slice_checksums.end())
+                    continue;
+                for (uint64_t b = 0; b < nblk[i] && b < it->second.size(); ++b) {
+                    memcpy(md5.data() + (first[i] + b) * 16, it->second[b].md5.data(), 16);
+                    crc[first[i] + b] = it->second[b].crc32;
+                    listed[first[i] + b] = true;
+                }
+            }
+            std::vector<const uint8_t *> sp = dev.ptrs(0, k);
+            check(p2g_verify_slices(codec_ctx(), sp.data(), k, bs, md5.data(), crc.data(), ok.data(),
+                                    P2G_DEVICE_PTRS));
+            for (uint64_t g = 0; g < k; ++g)
+                if (!ok[g] || !listed[g])
+                    damaged.push_back(g);
+        }
+        stats_.damaged_blocks = damaged.size();
+        if (damaged.empty()) {
+            stats_.ms_gpu = ms_since(t2);
+            stats_.ms_total = ms_since(t0);
+            return 0;
+        }
+        std::vector<RecoveryRef> recs = p.recovery_blocks;
+        std::stable_sort(recs.begin(), recs.end(),
+                         [](const RecoveryRef &a, const RecoveryRef &b) { return a.exponent < b.exponent; });
+        recs.erase(std::unique(recs.begin(), recs.end(),
+                               [](const RecoveryRef &a, const RecoveryRef &b) { return a.exponent == b.exponent; }),
+                   recs.end());
+        const uint64_t m = damaged.size();
+        if (recs.size() < m)
+            throw Par2Error("Insufficient recovery blocks: need " + std::to_string(m) + ", have " +
+                            std::to_string(recs.size()));
+        // the m lowest exponents' slices to the device, then the repair there
+        detail::DeviceSlices rdev(m, bs), out(m, bs);
+        std::vector<uint32_t> exps(m);
+        for (uint64_t q = 0; q < m; ++q) {
+            const std::vector<uint8_t> d = p.read_recovery(recs[q], 0, bs);
+            detail::cuda_check(cudaMemcpy(rdev.slice(q), d.data(), bs, cudaMemcpyHostToDevice),
+                               "cudaMemcpy (recovery slice)");
+            exps[q] = recs[q].exponent;
+        }
+        std::set<uint64_t> dset(damaged.begin(), damaged.end());
+        std::vector<const uint8_t *> present;
+        for (uint64_t g = 0; g < k; ++g)
+            if (!dset.count(g))
+                present.push_back(dev.slice(g));
+        std::vector<const uint8_t *> rp = rdev.ptrs(0, m);
+        std::vector<uint8_t *> op(m);
+        for (uint64_t q = 0; q < m; ++q)
+            op[q] = out.slice(q);
+        const int rc = p2g_repair(codec_ctx(), k, bs, damaged.data(), m, present.data(), exps.data(),
+                                  rp.data(), op.data(), P2G_DEVICE_PTRS);
+        if (rc == P2G_ESINGULAR)
+            throw Par2Error("Singular matrix");
+        check(rc);
+        for (uint64_t q = 0; q < m; ++q)
+            detail::cuda_check(cudaMemcpy(dev.slice(damaged[q]), out.slice(q), bs, cudaMemcpyDeviceToDevice),
+                               "cudaMemcpy (rebuilt slice)");
+        stats_.ms_gpu = ms_since(t2);
+        // rewrite the touched files and check them
+        const auto t3 = std::chrono::steady_clock::now();
+        for (size_t i = 0; i < p.files_in_order.size(); ++i) {
+            const FileInfo &f = p.files_in_order[i];
+            bool touched = false;
+            for (uint64_t b = 0; b < nblk[i] && !touched; ++b)
+                touched = dset.count(first[i] + b) > 0;
+            if (!touched)
+                continue;
+            std::vector<uint8_t> bytes(f.length);
+            if (f.length)
+                detail::cuda_check(cudaMemcpy(bytes.data(), dev.slice(first[i]), f.length, cudaMemcpyDeviceToHost),
+                                   "cudaMemcpy (repaired file)");
+            if (Md5::of(bytes.data(), bytes.size()) != f.hash)
+                throw Par2Error("Repaired file " + f.name + " does not match its MD5");
+            detail::write_file(dir_ / f.name, bytes.data(), bytes.size());
+            ++stats_.files_written;
+        }
+        stats_.ms_write = ms_since(t3);
+        stats_.ms_total = ms_since(t0);
+        return m;
+    }
+
+  private:
+    std::filesystem::path par2_, dir_;
+    PipelineStats stats_;
+};
+
+}  // namespace par2

@@ -1,0 +1,78 @@
+"""ctypes binding of include/par2format.h: create and repair of PAR2 sets
+from files (Par2Creator::create, Par2Repairer::repair of par2-rs) with the
+slices on the GPU.  Raises Par2FormatError with the library's message."""
+import ctypes
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "lib",
+                        "libpar2format.so")
+OK, ERROR, ESINGULAR, EINSUFFICIENT = 0, -1, -4, -8
+SCHEME_SINGLE, SCHEME_EXPONENTIAL = 0, 1
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("ms_scan", ctypes.c_double), ("ms_ingest", ctypes.c_double),
+                ("ms_gpu", ctypes.c_double), ("ms_write", ctypes.c_double),
+                ("ms_total", ctypes.c_double), ("block_size", ctypes.c_uint64),
+                ("data_blocks", ctypes.c_uint64), ("recovery_blocks", ctypes.c_uint64),
+                ("bytes_read", ctypes.c_uint64), ("damaged_blocks", ctypes.c_uint64),
+                ("files_written", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+SIGNATURES = [
+    ("p2f_create", [ctypes.POINTER(ctypes.c_char_p), ctypes.c_size_t, ctypes.c_char_p,
+                    ctypes.c_uint64, ctypes.c_float, ctypes.c_int, ctypes.POINTER(Stats)]),
+    ("p2f_repair", [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64),
+                    ctypes.POINTER(Stats)]),
+    ("p2f_last_error", []),
+]
+
+_lib = None
+
+
+class Par2FormatError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{msg} (code {code})")
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        from . import lib as gpu_lib
+
+        gpu_lib()  # libpar2gpu.so first: libpar2format.so links against it
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_char_p if name == "p2f_last_error" else ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != OK:
+        raise Par2FormatError(rc, lib().p2f_last_error().decode())
+
+
+def create(inputs, output=None, block_size=0, redundancy=5.0, scheme=SCHEME_EXPONENTIAL):
+    """Writes the set of `inputs` (paths); returns the call's Stats."""
+    arr = (ctypes.c_char_p * len(inputs))(*[os.fsencode(str(p)) for p in inputs])
+    st = Stats()
+    _check(lib().p2f_create(arr, len(inputs), os.fsencode(str(output)) if output else None,
+                            block_size, redundancy, scheme, ctypes.byref(st)))
+    return st
+
+
+def repair(par2_path, directory):
+    """Verifies and repairs the set's files in `directory`; returns
+    (slices rebuilt, Stats)."""
+    n = ctypes.c_uint64()
+    st = Stats()
+    _check(lib().p2f_repair(os.fsencode(str(par2_path)), os.fsencode(str(directory)),
+                            ctypes.byref(n), ctypes.byref(st)))
+    return n.value, st

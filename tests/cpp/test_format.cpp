@@ -1,4 +1,4 @@
-// Drives par2-rs_b200/host/par2_format.hpp for tests/test_format_cpp.py:
+// Drives par2-rs_b200/host/par2_format.hpp and par2_pipeline.hpp for tests/test_format_cpp.py:
 //
 //   test_format parse <file.par2>             parsed set as JSON (host only)
 //   test_format headers <dir> <block> <files...>
@@ -12,7 +12,7 @@
 #include <set>
 #include <string>
 
-#include "../../par2-rs_b200/host/par2_format.hpp"
+#include "../../par2-rs_b200/host/par2_pipeline.hpp"
 
 using namespace par2;
 namespace fs = std::filesystem;

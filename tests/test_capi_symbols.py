@@ -10,14 +10,25 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_symbols():
+def declared_symbols(prefix="p2g"):
     names = set()
     for fn in os.listdir(os.path.join(ROOT, "include")):
         if fn.endswith(".h"):
             text = open(os.path.join(ROOT, "include", fn)).read()
             text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-            names |= set(re.findall(r"\b(p2g_[a-z0-9_]+)\s*\(", text))
+            names |= set(re.findall(r"\b(%s_[a-z0-9_]+)\s*\(" % prefix, text))
     return names
+
+
+def test_format_library_exports_every_declared_symbol():
+    from par2gpu import format as fmt
+
+    L = ctypes.CDLL(fmt.LIB_PATH)
+    names = declared_symbols("p2f")
+    assert {"p2f_create", "p2f_repair", "p2f_last_error"} <= names
+    for n in sorted(names):
+        assert hasattr(L, n), f"missing export {n}"
+    assert names == {s[0] for s in fmt.SIGNATURES}
 
 
 def test_library_exports_every_declared_symbol():

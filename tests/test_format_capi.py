@@ -1,0 +1,72 @@
+"""The create / repair pipelines through their C ABI (include/par2format.h,
+libpar2format.so): Par2Creator::create and Par2Repairer::repair of par2-rs
+over files, with the slices streamed into device memory."""
+import os
+
+import numpy as np
+import pytest
+
+from par2gpu import format as fmt
+
+
+def make_files(d, sizes, seed):
+    rng = np.random.default_rng(seed)
+    names = []
+    for i, n in enumerate(sizes):
+        p = d / f"part{i}.bin"
+        p.write_bytes(rng.integers(0, 256, n, dtype=np.uint8).tobytes())
+        names.append(p)
+    return names
+
+
+def test_errors_without_work(tmp_path):
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.create([tmp_path / "missing.bin"])
+    assert ei.value.code == fmt.ERROR and "Input file does not exist" in str(ei.value)
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.create([])
+    assert "No input files" in str(ei.value)
+    (tmp_path / "a.bin").write_bytes(b"x" * 10)
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.create([tmp_path / "a.bin"], block_size=2050)
+    assert "multiple of 4" in str(ei.value)
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair(tmp_path / "none.par2", tmp_path)
+    assert ei.value.code == fmt.ERROR
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheme", [fmt.SCHEME_SINGLE, fmt.SCHEME_EXPONENTIAL])
+def test_create_damage_repair(tmp_path, scheme):
+    sizes = [0, 3, 100000, 1 << 20, (1 << 20) + 17, 5 * 65536, 777777]
+    files = make_files(tmp_path, sizes, 21)
+    orig = {p.name: p.read_bytes() for p in files}
+    # 53 slices of 64 KiB, 70 %: 38 recovery slices for the 32 damaged below
+    st = fmt.create(files, tmp_path / "set.par2", block_size=65536, redundancy=70, scheme=scheme)
+    assert st.bytes_read == sum(sizes) and st.block_size == 65536
+    assert st.data_blocks == sum((n + 65535) // 65536 for n in sizes)
+    assert st.recovery_blocks == (int(st.data_blocks * 65536 * 0.7) + 65535) // 65536 == 38
+    assert (tmp_path / "set.par2").exists()
+    n, st = fmt.repair(tmp_path / "set.par2", tmp_path)
+    assert n == 0 and st.damaged_blocks == 0
+    # a lost file, a truncated file and flipped bytes in a third
+    os.unlink(tmp_path / "part3.bin")
+    (tmp_path / "part4.bin").write_bytes(orig["part4.bin"][:200000])
+    b = bytearray(orig["part6.bin"])
+    b[12345] ^= 1
+    b[-1] ^= 0x80
+    (tmp_path / "part6.bin").write_bytes(bytes(b))
+    n, st = fmt.repair(tmp_path / "set.par2", tmp_path)
+    assert n == 16 + 14 + 2 and st.files_written == 3
+    for p in files:
+        assert p.read_bytes() == orig[p.name], p.name
+
+
+@pytest.mark.gpu
+def test_insufficient_recovery(tmp_path):
+    files = make_files(tmp_path, [1 << 20, 1 << 20], 22)
+    fmt.create(files, tmp_path / "s.par2", block_size=65536, redundancy=5)  # 2 slices
+    os.unlink(files[0])
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair(tmp_path / "s.par2", tmp_path)
+    assert ei.value.code == fmt.EINSUFFICIENT
