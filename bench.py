@@ -573,6 +573,76 @@ def run_tensor_alternative(args):
                       "encode_ms_at_bmma_peak": bitmacs / rate.value * 1e3}), flush=True)
 
 
+def run_create_files(args):
+    """Create and repair from files (p2f_create / p2f_repair): the large-encode
+    set as 4 files x 512 MiB on tmpfs (page cache), 1 MiB slices, 10 %
+    redundancy; then 200 slices of one file zeroed and repaired.  Beside it
+    the reference's CPU create path restated: whole-file MD5s of the files in
+    parallel, IFSC checksums slice by slice, the AVX2 encode (timed on the
+    48 KiB column sample of every slice and scaled to the slice size)."""
+    import shutil
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
+    from par2gpu import format as fmt
+
+    nfiles, fsize, bs, pct = 4, 512 << 20, 1 << 20, 10.0
+    base = "/dev/shm" if os.path.isdir("/dev/shm") and \
+        shutil.disk_usage("/dev/shm").free > 3 * nfiles * fsize else None
+    d = tempfile.mkdtemp(prefix="p2f_", dir=base)
+    try:
+        rng = np.random.default_rng(SEED + 9)
+        files = []
+        for i in range(nfiles):
+            p = os.path.join(d, f"file{i}.bin")
+            rng.integers(0, 256, fsize, dtype=np.uint8).tofile(p)
+            files.append(p)
+        # warm-up on a small set (device context, kernels, reader threads)
+        wp = os.path.join(d, "warm.bin")
+        rng.integers(0, 256, 8 << 20, dtype=np.uint8).tofile(wp)
+        for _ in range(max(1, args.warmup)):
+            fmt.create([wp], os.path.join(d, "warm.par2"), block_size=bs, redundancy=pct)
+        out = os.path.join(d, "set.par2")
+        st = fmt.create(files, out, block_size=bs, redundancy=pct)
+        total = nfiles * fsize
+        # damage: 200 slices of file 1 zeroed
+        with open(files[1], "r+b") as f:
+            f.write(bytes(200 * bs))
+        n, rst = fmt.repair(out, d)
+        res = {"workload": f"create_files: {nfiles} files x {fsize >> 20} MiB (tmpfs: "
+                           f"{base is not None}), {bs >> 20} MiB slices, {pct:g}% recovery; repair "
+                           "of 200 zeroed slices",
+               "create": dict(st.as_dict(), gbs=total / (st.ms_total * 1e-3) / 1e9),
+               "repair": dict(rst.as_dict(), rebuilt=n, gbs=total / (rst.ms_total * 1e-3) / 1e9)}
+        # the reference's CPU create path (restated; oracle = OpenSSL MD5, zlib CRC32)
+        from oracle import oracle
+
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        data = [np.fromfile(p, np.uint8) for p in files]
+        t_read = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(nfiles) as ex:
+            list(ex.map(oracle.md5, data))
+        t_md5 = time.perf_counter() - t0
+        slices = np.concatenate(data).reshape(-1, bs)
+        t0 = time.perf_counter()
+        oracle.hash_slices(slices)
+        t_ifsc = time.perf_counter() - t0
+        r = int(st.recovery_blocks)
+        gbs_enc, _, nbytes, _ = cpu_encode_rate(slices, slices.shape[0], bs, r, threads)
+        t_enc = total / (gbs_enc * 1e9)
+        t_cpu = t_read + t_md5 + t_ifsc + t_enc
+        res["cpu_baseline"] = {
+            "value": total / t_cpu / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"whole files for MD5 and IFSC; encode on the first "
+                      f"{CPU_SAMPLE_BYTES // 1024} KiB of every slice, scaled",
+            "s_read": t_read, "s_file_md5": t_md5, "s_ifsc": t_ifsc, "s_encode": t_enc}
+        print(json.dumps(res), flush=True)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def batched_sets(seed, nsets=256):
     """The batched configuration's set list: file sizes log-uniform on
     [64 KiB, 256 MiB], slice size uniform over {4, 16, 64, 256, 1024} KiB
@@ -848,7 +918,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large_encode",
                     choices=sorted(WORKLOADS) + sorted(HASH_WORKLOADS) +
-                    ["verify_repair", "invert", "tensor_alternative", "batched", "serving"])
+                    ["verify_repair", "invert", "tensor_alternative", "create_files", "batched",
+                     "serving"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the heuristic tile shape instead of the autotuned one")
     ap.add_argument("--quick", action="store_true",
@@ -865,6 +936,9 @@ def main():
         return
     if args.workload == "tensor_alternative":
         run_tensor_alternative(args)
+        return
+    if args.workload == "create_files":
+        run_create_files(args)
         return
     if args.workload == "batched":
         run_batched(args)

@@ -88,41 +88,54 @@ class Md5 {
 
   private:
     static uint32_t rotl(uint32_t x, int s) { return (x << s) | (x >> (32 - s)); }
+    // one RFC 1321 block: four rounds of 16 steps, T[i] = floor(2^32 |sin(i + 1)|)
     void block(const uint8_t *p)
     {
-        // RFC 1321 3.4: T[i] = floor(2^32 |sin(i + 1)|), per-round shifts
-        static const uint32_t T[64] = {
-            0xd76aa478, 0xe8c7b756, 0x242070db, 0xc1bdceee, 0xf57c0faf, 0x4787c62a, 0xa8304613,
-            0xfd469501, 0x698098d8, 0x8b44f7af, 0xffff5bb1, 0x895cd7be, 0x6b901122, 0xfd987193,
-            0xa679438e, 0x49b40821, 0xf61e2562, 0xc040b340, 0x265e5a51, 0xe9b6c7aa, 0xd62f105d,
-            0x02441453, 0xd8a1e681, 0xe7d3fbc8, 0x21e1cde6, 0xc33707d6, 0xf4d50d87, 0x455a14ed,
-            0xa9e3e905, 0xfcefa3f8, 0x676f02d9, 0x8d2a4c8a, 0xfffa3942, 0x8771f681, 0x6d9d6122,
-            0xfde5380c, 0xa4beea44, 0x4bdecfa9, 0xf6bb4b60, 0xbebfbc70, 0x289b7ec6, 0xeaa127fa,
-            0xd4ef3085, 0x04881d05, 0xd9d4d039, 0xe6db99e5, 0x1fa27cf8, 0xc4ac5665, 0xf4292244,
-            0x432aff97, 0xab9423a7, 0xfc93a039, 0x655b59c3, 0x8f0ccc92, 0xffeff47d, 0x85845dd1,
-            0x6fa87e4f, 0xfe2ce6e0, 0xa3014314, 0x4e0811a1, 0xf7537e82, 0xbd3af235, 0x2ad7d2bb,
-            0xeb86d391};
-        static const int R[4][4] = {{7, 12, 17, 22}, {5, 9, 14, 20}, {4, 11, 16, 23}, {6, 10, 15, 21}};
         uint32_t x[16];
-        for (int i = 0; i < 16; ++i)
-            x[i] = uint32_t(p[4 * i]) | uint32_t(p[4 * i + 1]) << 8 | uint32_t(p[4 * i + 2]) << 16 |
-                   uint32_t(p[4 * i + 3]) << 24;
+        memcpy(x, p, 64);  // little-endian host
         uint32_t a = s_[0], b = s_[1], c = s_[2], d = s_[3];
-        for (int i = 0; i < 64; ++i) {
-            uint32_t f;
-            int g;
-            switch (i >> 4) {
-            case 0: f = (b & c) | (~b & d); g = i; break;
-            case 1: f = (b & d) | (c & ~d); g = (5 * i + 1) & 15; break;
-            case 2: f = b ^ c ^ d; g = (3 * i + 5) & 15; break;
-            default: f = c ^ (b | ~d); g = (7 * i) & 15; break;
-            }
-            const uint32_t t = d;
-            d = c;
-            c = b;
-            b = b + rotl(a + f + x[g] + T[i], R[i >> 4][i & 3]);
-            a = t;
-        }
+#define P2F_STEP(F, a, b, c, d, k, s, t) a = b + rotl(a + F(b, c, d) + x[k] + t, s)
+#define P2F_F(b, c, d) (d ^ (b & (c ^ d)))
+#define P2F_G(b, c, d) (c ^ (d & (b ^ c)))
+#define P2F_H(b, c, d) (b ^ c ^ d)
+#define P2F_I(b, c, d) (c ^ (b | ~d))
+        P2F_STEP(P2F_F, a, b, c, d, 0, 7, 0xd76aa478);  P2F_STEP(P2F_F, d, a, b, c, 1, 12, 0xe8c7b756);
+        P2F_STEP(P2F_F, c, d, a, b, 2, 17, 0x242070db); P2F_STEP(P2F_F, b, c, d, a, 3, 22, 0xc1bdceee);
+        P2F_STEP(P2F_F, a, b, c, d, 4, 7, 0xf57c0faf);  P2F_STEP(P2F_F, d, a, b, c, 5, 12, 0x4787c62a);
+        P2F_STEP(P2F_F, c, d, a, b, 6, 17, 0xa8304613); P2F_STEP(P2F_F, b, c, d, a, 7, 22, 0xfd469501);
+        P2F_STEP(P2F_F, a, b, c, d, 8, 7, 0x698098d8);  P2F_STEP(P2F_F, d, a, b, c, 9, 12, 0x8b44f7af);
+        P2F_STEP(P2F_F, c, d, a, b, 10, 17, 0xffff5bb1); P2F_STEP(P2F_F, b, c, d, a, 11, 22, 0x895cd7be);
+        P2F_STEP(P2F_F, a, b, c, d, 12, 7, 0x6b901122); P2F_STEP(P2F_F, d, a, b, c, 13, 12, 0xfd987193);
+        P2F_STEP(P2F_F, c, d, a, b, 14, 17, 0xa679438e); P2F_STEP(P2F_F, b, c, d, a, 15, 22, 0x49b40821);
+        P2F_STEP(P2F_G, a, b, c, d, 1, 5, 0xf61e2562);  P2F_STEP(P2F_G, d, a, b, c, 6, 9, 0xc040b340);
+        P2F_STEP(P2F_G, c, d, a, b, 11, 14, 0x265e5a51); P2F_STEP(P2F_G, b, c, d, a, 0, 20, 0xe9b6c7aa);
+        P2F_STEP(P2F_G, a, b, c, d, 5, 5, 0xd62f105d);  P2F_STEP(P2F_G, d, a, b, c, 10, 9, 0x02441453);
+        P2F_STEP(P2F_G, c, d, a, b, 15, 14, 0xd8a1e681); P2F_STEP(P2F_G, b, c, d, a, 4, 20, 0xe7d3fbc8);
+        P2F_STEP(P2F_G, a, b, c, d, 9, 5, 0x21e1cde6);  P2F_STEP(P2F_G, d, a, b, c, 14, 9, 0xc33707d6);
+        P2F_STEP(P2F_G, c, d, a, b, 3, 14, 0xf4d50d87); P2F_STEP(P2F_G, b, c, d, a, 8, 20, 0x455a14ed);
+        P2F_STEP(P2F_G, a, b, c, d, 13, 5, 0xa9e3e905); P2F_STEP(P2F_G, d, a, b, c, 2, 9, 0xfcefa3f8);
+        P2F_STEP(P2F_G, c, d, a, b, 7, 14, 0x676f02d9); P2F_STEP(P2F_G, b, c, d, a, 12, 20, 0x8d2a4c8a);
+        P2F_STEP(P2F_H, a, b, c, d, 5, 4, 0xfffa3942);  P2F_STEP(P2F_H, d, a, b, c, 8, 11, 0x8771f681);
+        P2F_STEP(P2F_H, c, d, a, b, 11, 16, 0x6d9d6122); P2F_STEP(P2F_H, b, c, d, a, 14, 23, 0xfde5380c);
+        P2F_STEP(P2F_H, a, b, c, d, 1, 4, 0xa4beea44);  P2F_STEP(P2F_H, d, a, b, c, 4, 11, 0x4bdecfa9);
+        P2F_STEP(P2F_H, c, d, a, b, 7, 16, 0xf6bb4b60); P2F_STEP(P2F_H, b, c, d, a, 10, 23, 0xbebfbc70);
+        P2F_STEP(P2F_H, a, b, c, d, 13, 4, 0x289b7ec6); P2F_STEP(P2F_H, d, a, b, c, 0, 11, 0xeaa127fa);
+        P2F_STEP(P2F_H, c, d, a, b, 3, 16, 0xd4ef3085); P2F_STEP(P2F_H, b, c, d, a, 6, 23, 0x04881d05);
+        P2F_STEP(P2F_H, a, b, c, d, 9, 4, 0xd9d4d039);  P2F_STEP(P2F_H, d, a, b, c, 12, 11, 0xe6db99e5);
+        P2F_STEP(P2F_H, c, d, a, b, 15, 16, 0x1fa27cf8); P2F_STEP(P2F_H, b, c, d, a, 2, 23, 0xc4ac5665);
+        P2F_STEP(P2F_I, a, b, c, d, 0, 6, 0xf4292244);  P2F_STEP(P2F_I, d, a, b, c, 7, 10, 0x432aff97);
+        P2F_STEP(P2F_I, c, d, a, b, 14, 15, 0xab9423a7); P2F_STEP(P2F_I, b, c, d, a, 5, 21, 0xfc93a039);
+        P2F_STEP(P2F_I, a, b, c, d, 12, 6, 0x655b59c3); P2F_STEP(P2F_I, d, a, b, c, 3, 10, 0x8f0ccc92);
+        P2F_STEP(P2F_I, c, d, a, b, 10, 15, 0xffeff47d); P2F_STEP(P2F_I, b, c, d, a, 1, 21, 0x85845dd1);
+        P2F_STEP(P2F_I, a, b, c, d, 8, 6, 0x6fa87e4f);  P2F_STEP(P2F_I, d, a, b, c, 15, 10, 0xfe2ce6e0);
+        P2F_STEP(P2F_I, c, d, a, b, 6, 15, 0xa3014314); P2F_STEP(P2F_I, b, c, d, a, 13, 21, 0x4e0811a1);
+        P2F_STEP(P2F_I, a, b, c, d, 4, 6, 0xf7537e82);  P2F_STEP(P2F_I, d, a, b, c, 11, 10, 0xbd3af235);
+        P2F_STEP(P2F_I, c, d, a, b, 2, 15, 0x2ad7d2bb); P2F_STEP(P2F_I, b, c, d, a, 9, 21, 0xeb86d391);
+#undef P2F_STEP
+#undef P2F_F
+#undef P2F_G
+#undef P2F_H
+#undef P2F_I
         s_[0] += a;
         s_[1] += b;
         s_[2] += c;

@@ -84,6 +84,7 @@ struct IngestJob {
     std::filesystem::path path;
     uint8_t *dst = nullptr;   // device: the file's first slice
     uint64_t length = 0;      // bytes to read (file length)
+    bool hash = true;         // fold the bytes into md5
     FileHash md5{};           // out: MD5 of what was read
     bool ok = false;          // out: the file existed and had `length` bytes
 };
@@ -119,7 +120,8 @@ inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads)
                     const size_t n = fread(buf[b], 1, std::min<uint64_t>(kChunk, job.length - off), f);
                     if (n == 0)
                         break;
-                    h.update(buf[b], n);
+                    if (job.hash)
+                        h.update(buf[b], n);
                     cuda_check(cudaMemcpyAsync(job.dst + off, buf[b], n, cudaMemcpyHostToDevice, st),
                                "cudaMemcpyAsync");
                     cuda_check(cudaEventRecord(ev[b], st), "cudaEventRecord");
@@ -183,6 +185,21 @@ inline void write_file(const std::filesystem::path &p, const uint8_t *d, size_t 
         throw Par2Error("Failed to write " + p.string());
     }
     fclose(f);
+}
+
+// fn(i) for i in [0, n) on the host's threads
+template <class F> void parallel_for(size_t n, F fn)
+{
+    const size_t nt = std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency()));
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (size_t i; (i = next.fetch_add(1)) < n;)
+                fn(i);
+        });
+    for (auto &th : pool)
+        th.join();
 }
 
 }  // namespace detail
@@ -354,13 +371,40 @@ class Par2Creator {
             index.path = output_;
             vols.insert(vols.begin(), index);
         }
+        // RecvSlic packets (header, exponent, slice; bs is a multiple of 4, so
+        // no padding): the headers' MD5s in parallel, the bodies written from
+        // the recovery buffer in place
+        std::vector<std::array<uint8_t, 68>> head(r);
+        detail::parallel_for(r, [&](size_t e) {
+            uint8_t *hd = head[e].data();
+            const uint8_t ex[4] = {static_cast<uint8_t>(e), static_cast<uint8_t>(e >> 8),
+                                   static_cast<uint8_t>(e >> 16), static_cast<uint8_t>(e >> 24)};
+            Md5 h;
+            h.update(set_id.data(), 16);
+            h.update(packet_types::RECV_SLICE.data(), 16);
+            h.update(ex, 4);
+            h.update(rec.data() + e * bs, bs);
+            const FileHash md5 = h.finalize();
+            const uint64_t len = 64 + 4 + bs;
+            memcpy(hd, kPar2Magic, 8);
+            for (int i = 0; i < 8; ++i)
+                hd[8 + i] = static_cast<uint8_t>(len >> (8 * i));
+            memcpy(hd + 16, md5.data(), 16);
+            memcpy(hd + 32, set_id.data(), 16);
+            memcpy(hd + 48, packet_types::RECV_SLICE.data(), 16);
+            memcpy(hd + 64, ex, 4);
+        });
         std::vector<std::filesystem::path> written;
         for (const VolumeInfo &v : vols) {
-            std::vector<uint8_t> out = common;
+            FILE *f = fopen(v.path.string().c_str(), "wb");
+            bool ok = f && fwrite(common.data(), 1, common.size(), f) == common.size();
             for (uint32_t e : v.exponents)
-                write_packet(out, packet_types::RECV_SLICE, set_id,
-                             recovery_body(e, rec.data() + static_cast<size_t>(e) * bs, bs));
-            detail::write_file(v.path, out.data(), out.size());
+                ok = ok && fwrite(head[e].data(), 1, 68, f) == 68 &&
+                     fwrite(rec.data() + static_cast<size_t>(e) * bs, 1, bs, f) == bs;
+            if (f)
+                ok = fclose(f) == 0 && ok;
+            if (!ok)
+                throw Par2Error("Failed to write " + v.path.string());
             written.push_back(v.path);
         }
         stats_.files_written = written.size();
@@ -382,9 +426,8 @@ class Par2Creator {
 // Verification and repair of the files of a set in `dir`: every slice is
 // checked against its IFSC entry on the GPU (a missing or short file counts
 // as damaged where it lacks data), the damaged slices are rebuilt from the m
-// lowest recovery exponents (repair.rs:537-604) and the touched files are
-// rewritten; finally every rewritten file's MD5 is checked against its
-// FileDesc entry.
+// lowest recovery exponents (repair.rs:537-604), checked again against
+// their IFSC entries, and the touched files are rewritten.
 class Par2Repairer {
   public:
     Par2Repairer(std::filesystem::path par2, std::filesystem::path dir)
@@ -422,15 +465,17 @@ class Par2Repairer {
             jobs[i].path = dir_ / p.files_in_order[i].name;
             jobs[i].dst = k ? dev.slice(first[i]) : nullptr;
             jobs[i].length = p.files_in_order[i].length;
+            jobs[i].hash = false;  // the slices are verified on the device
         }
         stats_.bytes_read = detail::ingest(jobs, detail::reader_threads(jobs.size()));
         stats_.ms_ingest = ms_since(t1);
         const auto t2 = std::chrono::steady_clock::now();
         // per-slice verification on the device
         std::vector<uint64_t> damaged;
+        std::vector<uint8_t> md5(k * 16, 0);
+        std::vector<uint32_t> crc(k, 0);
         if (k) {
-            std::vector<uint8_t> md5(k * 16, 0), ok(k, 0);
-            std::vector<uint32_t> crc(k, 0);
+            std::vector<uint8_t> ok(k, 0);
             std::vector<bool> listed(k, false);
             for (size_t i = 0; i < p.files_in_order.size(); ++i) {
                 const auto it = p.slice_checksums.find(p.files_in_order[i].file_id);
@@ -491,6 +536,25 @@ class Par2Repairer {
         for (uint64_t q = 0; q < m; ++q)
             detail::cuda_check(cudaMemcpy(dev.slice(damaged[q]), out.slice(q), bs, cudaMemcpyDeviceToDevice),
                                "cudaMemcpy (rebuilt slice)");
+        // the rebuilt slices against their IFSC entries (the post-repair
+        // verification of repair.rs:1062-1096, per slice)
+        {
+            std::vector<uint8_t> wmd5(m * 16), ok(m, 0);
+            std::vector<uint32_t> wcrc(m);
+            for (uint64_t q = 0; q < m; ++q) {
+                memcpy(wmd5.data() + q * 16, md5.data() + damaged[q] * 16, 16);
+                wcrc[q] = crc[damaged[q]];
+            }
+            std::vector<const uint8_t *> rp2(m);
+            for (uint64_t q = 0; q < m; ++q)
+                rp2[q] = dev.slice(damaged[q]);
+            check(p2g_verify_slices(codec_ctx(), rp2.data(), m, bs, wmd5.data(), wcrc.data(), ok.data(),
+                                    P2G_DEVICE_PTRS));
+            for (uint64_t q = 0; q < m; ++q)
+                if (!ok[q])
+                    throw Par2Error("Rebuilt slice " + std::to_string(damaged[q]) +
+                                    " does not match its checksums");
+        }
         stats_.ms_gpu = ms_since(t2);
         // rewrite the touched files and check them
         const auto t3 = std::chrono::steady_clock::now();
@@ -505,8 +569,6 @@ class Par2Repairer {
             if (f.length)
                 detail::cuda_check(cudaMemcpy(bytes.data(), dev.slice(first[i]), f.length, cudaMemcpyDeviceToHost),
                                    "cudaMemcpy (repaired file)");
-            if (Md5::of(bytes.data(), bytes.size()) != f.hash)
-                throw Par2Error("Repaired file " + f.name + " does not match its MD5");
             detail::write_file(dir_ / f.name, bytes.data(), bytes.size());
             ++stats_.files_written;
         }
