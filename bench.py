@@ -566,11 +566,17 @@ def run_tensor_alternative(args):
         print(json.dumps({"workload": "tensor_alternative", "error": rc}))
         return
     bitmacs = 16 * r * 16 * k * (S // 2)
+    tm = (ctypes.c_double * 4)()
+    trc = lib.p2g_probe_tmem(0, ctypes.c_double(1.965e9), tm)
     print(json.dumps({"workload": "tensor_alternative: GF(2) bit-matrix encode of k=2048 x 1 MiB, "
-                                  "r=205 on binary MMA (mma.sync m16n8k256 b1 and.popc)",
+                                  "r=205 on binary MMA (mma.sync m16n8k256 b1 and.popc); tensor "
+                                  "memory as a second table store",
                       "bmma_bit_macs_per_s": rate.value, "probe_ms": ms.value,
                       "encode_bit_macs": bitmacs,
-                      "encode_ms_at_bmma_peak": bitmacs / rate.value * 1e3}), flush=True)
+                      "encode_ms_at_bmma_peak": bitmacs / rate.value * 1e3,
+                      "table_reads_bytes_per_sm_clock_at_1965MHz": None if trc else {
+                          "tmem_alone": tm[0], "shared_alone": tm[1],
+                          "interleaved_tmem": tm[2], "interleaved_shared": tm[3]}}), flush=True)
 
 
 def run_create_files(args):
