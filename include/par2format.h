@@ -20,6 +20,8 @@ extern "C" {
 #define P2F_ERROR (-1)          /* Par2Error::InvalidFormat / Io: see p2f_last_error */
 #define P2F_ESINGULAR (-4)      /* Par2Error::RepairFailed("Singular matrix") */
 #define P2F_EINSUFFICIENT (-8)  /* Par2Error::InsufficientRecovery (error.rs:5-39) */
+#define P2F_ECANCELLED (-9)     /* Par2Error::Cancelled: "PAR2 operation cancelled" */
+#define P2F_EDAMAGED (-10)      /* RepairFailed("Files are damaged and repair was not requested") */
 
 #define P2F_SCHEME_SINGLE 0       /* VolumeScheme::Single (volumes.rs:27-31) */
 #define P2F_SCHEME_EXPONENTIAL 1  /* VolumeScheme::Exponential: 1, 2, 4 ... slices per file */
@@ -44,6 +46,26 @@ int p2f_create(const char *const *inputs, size_t n, const char *output, uint64_t
  * in place.  *rebuilt (may be NULL) receives the number of slices rebuilt,
  * 0 when every slice was intact. */
 int p2f_repair(const char *par2_path, const char *dir, uint64_t *rebuilt, p2f_stats *stats);
+
+/* Par2Operation (lib.rs:76-81) passed to the progress callback */
+#define P2F_OP_SCANNING 0
+#define P2F_OP_LOADING 1
+#define P2F_OP_VERIFYING 2
+#define P2F_OP_REPAIRING 3
+typedef void (*p2f_progress_fn)(void *user, int operation, uint64_t current, uint64_t total);
+
+/* Par2Repairer::repair_with_callbacks_cancellable (lib.rs:196-351):
+ *   do_repair  0: verify only -- any damage returns P2F_EDAMAGED
+ *   purge      1: delete the set's .par2 files after a verified or repaired set
+ *   progress   optional (operation, current, total) callback, called on this thread
+ *   cancel     optional flag; set it non-zero from any thread to stop at the next
+ *              safe point (P2F_ECANCELLED).  Rebuilt files are written to
+ *              <name>.par2tmp and renamed into place only after all of them are
+ *              written, so a cancellation or an error before that leaves every
+ *              data file unchanged; a cancellation after it skips the purge. */
+int p2f_repair_ex(const char *par2_path, const char *dir, int do_repair, int purge,
+                  p2f_progress_fn progress, void *user, const volatile int32_t *cancel,
+                  uint64_t *rebuilt, p2f_stats *stats);
 
 const char *p2f_last_error(void);
 

@@ -12,6 +12,10 @@ thread_local std::string g_error;
 int fail(const std::exception &e)
 {
     g_error = e.what();
+    if (dynamic_cast<const par2::Cancelled *>(&e))
+        return P2F_ECANCELLED;
+    if (g_error.find("repair was not requested") != std::string::npos)
+        return P2F_EDAMAGED;
     if (g_error.find("Singular matrix") != std::string::npos)
         return P2F_ESINGULAR;
     if (g_error.find("Insufficient recovery") != std::string::npos)
@@ -78,6 +82,32 @@ int p2f_repair(const char *par2_path, const char *dir, uint64_t *rebuilt, p2f_st
         if (!par2_path || !dir)
             throw par2::Par2Error("p2f_repair: null path");
         par2::Par2Repairer r(par2_path, dir);
+        const uint64_t n = r.repair();
+        if (rebuilt)
+            *rebuilt = n;
+        fill(stats, r.stats());
+        return P2F_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+int p2f_repair_ex(const char *par2_path, const char *dir, int do_repair, int purge,
+                  p2f_progress_fn progress, void *user, const volatile int32_t *cancel,
+                  uint64_t *rebuilt, p2f_stats *stats)
+{
+    g_error.clear();
+    try {
+        if (!par2_path || !dir)
+            throw par2::Par2Error("p2f_repair_ex: null path");
+        par2::Par2Repairer r(par2_path, dir);
+        r.with_repair(do_repair != 0).with_purge(purge != 0);
+        if (progress)
+            r.with_progress([progress, user](par2::Par2Operation op, uint64_t cur, uint64_t tot) {
+                progress(user, static_cast<int>(op), cur, tot);
+            });
+        if (cancel)
+            r.with_cancel([cancel] { return *cancel != 0; });
         const uint64_t n = r.repair();
         if (rebuilt)
             *rebuilt = n;

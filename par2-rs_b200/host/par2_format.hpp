@@ -409,6 +409,7 @@ class Par2File {
     std::vector<RecoveryRef> recovery_blocks;
     std::map<FileHash, std::vector<SliceChecksum>> slice_checksums;
     std::vector<FileHash> main_order;       // the Main packet's File ID list
+    std::vector<std::filesystem::path> set_files;  // this file and the volumes read with it
 
     // Parses `path`, then every other *.par2 in its directory with the same
     // recovery set ID (parser.rs:181-547).  Packets with a bad magic, length or
@@ -430,6 +431,7 @@ class Par2File {
         for (const auto &d : deferred)
             if (d.second >= 68)
                 p.add_recovery(path, d.first);
+        p.set_files.push_back(path);
         if (scan_volumes) {
             std::filesystem::path dir = path.parent_path();
             if (dir.empty())
@@ -450,6 +452,7 @@ class Par2File {
                     vol.scan(v, file_size(v), false, nullptr);
                     p.recovery_blocks.insert(p.recovery_blocks.end(), vol.recovery_blocks.begin(),
                                              vol.recovery_blocks.end());
+                    p.set_files.push_back(v);
                 }
             }
         }

@@ -17,6 +17,7 @@
 
 #include <atomic>
 #include <chrono>
+#include <functional>
 #include <set>
 #include <thread>
 
@@ -49,14 +50,22 @@ inline void cuda_check(cudaError_t e, const char *what)
     }
 }
 
-// Device buffer of k zero-padded slices of bs bytes.
+// Device buffer of k zero-padded slices of bs bytes.  The zero fill has
+// finished when the constructor returns: the buffer is then written from
+// non-blocking streams (the readers', the codec context's), which do not
+// order themselves after work on the default stream.
 class DeviceSlices {
   public:
     DeviceSlices(uint64_t k, uint64_t bs) : k_(k), bs_(bs)
     {
         if (k && bs) {
             cuda_check(cudaMalloc(&p_, k * bs), "cudaMalloc (slices)");
-            cuda_check(cudaMemset(p_, 0, k * bs), "cudaMemset (slices)");
+            cudaStream_t st = nullptr;
+            cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+            const cudaError_t e1 = cudaMemsetAsync(p_, 0, k * bs, st);
+            const cudaError_t e2 = cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+            cuda_check(e1 != cudaSuccess ? e1 : e2, "cudaMemsetAsync (slices)");
         }
     }
     ~DeviceSlices()
@@ -91,8 +100,13 @@ struct IngestJob {
 
 // Reads every job's file into device memory with whole-file MD5s, `threads`
 // files at a time.
-inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads)
+// true when the caller asked to stop (polled between phases and read chunks)
+using CancelFn = std::function<bool()>;
+
+inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads,
+                       const CancelFn *cancel = nullptr)
 {
+    auto cancelled = [&] { return cancel && *cancel && (*cancel)(); };
     constexpr size_t kChunk = 8u << 20;
     std::atomic<size_t> next{0};
     std::atomic<uint64_t> total{0};
@@ -107,7 +121,7 @@ inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads)
                 cuda_check(cudaMallocHost(reinterpret_cast<void **>(&buf[b]), kChunk), "cudaMallocHost");
                 cuda_check(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming), "cudaEventCreate");
             }
-            for (size_t j; (j = next.fetch_add(1)) < jobs.size();) {
+            for (size_t j; !cancelled() && (j = next.fetch_add(1)) < jobs.size();) {
                 IngestJob &job = jobs[j];
                 FILE *f = fopen(job.path.string().c_str(), "rb");
                 if (!f)
@@ -115,7 +129,7 @@ inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads)
                 Md5 h;
                 uint64_t off = 0;
                 int b = 0;
-                while (off < job.length) {
+                while (off < job.length && !cancelled()) {
                     cuda_check(cudaEventSynchronize(ev[b]), "cudaEventSynchronize");
                     const size_t n = fread(buf[b], 1, std::min<uint64_t>(kChunk, job.length - off), f);
                     if (n == 0)
@@ -423,16 +437,50 @@ class Par2Creator {
     PipelineStats stats_;
 };
 
-// Verification and repair of the files of a set in `dir`: every slice is
-// checked against its IFSC entry on the GPU (a missing or short file counts
-// as damaged where it lacks data), the damaged slices are rebuilt from the m
-// lowest recovery exponents (repair.rs:537-604), checked again against
-// their IFSC entries, and the touched files are rewritten.
+// Par2Operation (lib.rs:76-81) and the progress callback (operation, current, total)
+enum class Par2Operation { Scanning = 0, Loading = 1, Verifying = 2, Repairing = 3 };
+using ProgressCallback = std::function<void(Par2Operation, uint64_t, uint64_t)>;
+
+struct Cancelled : Par2Error {
+    Cancelled() : Par2Error("PAR2 operation cancelled") {}
+};
+
+// Verification and repair of the files of a set in `dir`
+// (Par2Repairer::repair_with_callbacks_cancellable, lib.rs:196-351): every
+// slice is checked against its IFSC entry on the GPU (a missing or short file
+// counts as damaged where it lacks data); without do_repair any damage is an
+// error; otherwise the damaged slices are rebuilt from the m lowest recovery
+// exponents (repair.rs:537-604) and checked again against their IFSC
+// entries, every touched file is written to `<name>.par2tmp` and only then
+// are all of them renamed into place (repair.rs:54-110), so that an error or
+// a cancellation before the commit leaves every data file as it was.  With
+// purge, the set's .par2 files are deleted after a verified or repaired set.
+// The cancel flag is checked between phases and between read chunks.
 class Par2Repairer {
   public:
     Par2Repairer(std::filesystem::path par2, std::filesystem::path dir)
         : par2_(std::move(par2)), dir_(std::move(dir))
     {
+    }
+    Par2Repairer &with_repair(bool do_repair)
+    {
+        do_repair_ = do_repair;
+        return *this;
+    }
+    Par2Repairer &with_purge(bool purge)
+    {
+        purge_ = purge;
+        return *this;
+    }
+    Par2Repairer &with_progress(ProgressCallback cb)
+    {
+        progress_ = std::move(cb);
+        return *this;
+    }
+    Par2Repairer &with_cancel(detail::CancelFn is_cancelled)
+    {
+        cancel_ = std::move(is_cancelled);
+        return *this;
     }
     const PipelineStats &stats() const { return stats_; }
 
@@ -442,7 +490,10 @@ class Par2Repairer {
         using detail::ms_since;
         const auto t0 = std::chrono::steady_clock::now();
         stats_ = PipelineStats();
+        check_cancel();
+        report(Par2Operation::Loading, 0, 100);
         Par2File p = Par2File::load(par2_);
+        report(Par2Operation::Loading, 100, 100);
         const uint64_t bs = p.block_size;
         std::vector<uint64_t> first, nblk;
         uint64_t k = 0;
@@ -457,7 +508,10 @@ class Par2Repairer {
         stats_.data_blocks = k;
         stats_.recovery_blocks = p.recovery_blocks.size();
         stats_.ms_scan = ms_since(t0);
+        check_cancel();
+        // the files into device slices (no hashing: the slices are verified)
         const auto t1 = std::chrono::steady_clock::now();
+        report(Par2Operation::Verifying, 0, 100);
         codec_ctx();
         detail::DeviceSlices dev(k, bs);
         std::vector<detail::IngestJob> jobs(p.files_in_order.size());
@@ -465,12 +519,13 @@ class Par2Repairer {
             jobs[i].path = dir_ / p.files_in_order[i].name;
             jobs[i].dst = k ? dev.slice(first[i]) : nullptr;
             jobs[i].length = p.files_in_order[i].length;
-            jobs[i].hash = false;  // the slices are verified on the device
+            jobs[i].hash = false;
         }
-        stats_.bytes_read = detail::ingest(jobs, detail::reader_threads(jobs.size()));
+        stats_.bytes_read = detail::ingest(jobs, detail::reader_threads(jobs.size()), &cancel_);
+        check_cancel();
         stats_.ms_ingest = ms_since(t1);
-        const auto t2 = std::chrono::steady_clock::now();
         // per-slice verification on the device
+        const auto t2 = std::chrono::steady_clock::now();
         std::vector<uint64_t> damaged;
         std::vector<uint8_t> md5(k * 16, 0);
         std::vector<uint32_t> crc(k, 0);
@@ -494,12 +549,28 @@ class Par2Repairer {
                 if (!ok[g] || !listed[g])
                     damaged.push_back(g);
         }
+        // a file longer than its FileDesc length: its last slice is rebuilt so
+        // that the file is rewritten at its length
+        for (size_t i = 0; i < jobs.size(); ++i) {
+            std::error_code ec;
+            const uint64_t sz = std::filesystem::file_size(jobs[i].path, ec);
+            const uint64_t last = first[i] + nblk[i] - 1;
+            if (!ec && nblk[i] && sz > p.files_in_order[i].length &&
+                !std::binary_search(damaged.begin(), damaged.end(), last))
+                damaged.insert(std::lower_bound(damaged.begin(), damaged.end(), last), last);
+        }
+        report(Par2Operation::Verifying, 100, 100);
         stats_.damaged_blocks = damaged.size();
+        stats_.ms_gpu = ms_since(t2);
         if (damaged.empty()) {
-            stats_.ms_gpu = ms_since(t2);
-            stats_.ms_total = ms_since(t0);
+            finish(p, t0);
             return 0;
         }
+        if (!do_repair_)
+            throw Par2Error("Files are damaged and repair was not requested");
+        check_cancel();
+        report(Par2Operation::Repairing, 0, 100);
+        const auto t3 = std::chrono::steady_clock::now();
         std::vector<RecoveryRef> recs = p.recovery_blocks;
         std::stable_sort(recs.begin(), recs.end(),
                          [](const RecoveryRef &a, const RecoveryRef &b) { return a.exponent < b.exponent; });
@@ -519,6 +590,7 @@ class Par2Repairer {
                                "cudaMemcpy (recovery slice)");
             exps[q] = recs[q].exponent;
         }
+        check_cancel();
         std::set<uint64_t> dset(damaged.begin(), damaged.end());
         std::vector<const uint8_t *> present;
         for (uint64_t g = 0; g < k; ++g)
@@ -536,49 +608,95 @@ class Par2Repairer {
         for (uint64_t q = 0; q < m; ++q)
             detail::cuda_check(cudaMemcpy(dev.slice(damaged[q]), out.slice(q), bs, cudaMemcpyDeviceToDevice),
                                "cudaMemcpy (rebuilt slice)");
+        // device-to-device copies return before they finish; the check below
+        // runs on the codec context's own stream
+        detail::cuda_check(cudaStreamSynchronize(cudaStreamLegacy), "cudaStreamSynchronize");
         // the rebuilt slices against their IFSC entries (the post-repair
-        // verification of repair.rs:1062-1096, per slice)
+        // verification of lib.rs:302-325, per slice)
         {
             std::vector<uint8_t> wmd5(m * 16), ok(m, 0);
             std::vector<uint32_t> wcrc(m);
+            std::vector<const uint8_t *> rp2(m);
             for (uint64_t q = 0; q < m; ++q) {
                 memcpy(wmd5.data() + q * 16, md5.data() + damaged[q] * 16, 16);
                 wcrc[q] = crc[damaged[q]];
-            }
-            std::vector<const uint8_t *> rp2(m);
-            for (uint64_t q = 0; q < m; ++q)
                 rp2[q] = dev.slice(damaged[q]);
+            }
             check(p2g_verify_slices(codec_ctx(), rp2.data(), m, bs, wmd5.data(), wcrc.data(), ok.data(),
                                     P2G_DEVICE_PTRS));
             for (uint64_t q = 0; q < m; ++q)
                 if (!ok[q])
-                    throw Par2Error("Rebuilt slice " + std::to_string(damaged[q]) +
-                                    " does not match its checksums");
+                    throw Par2Error("Repair completed but verification failed - files may still be damaged");
         }
-        stats_.ms_gpu = ms_since(t2);
-        // rewrite the touched files and check them
-        const auto t3 = std::chrono::steady_clock::now();
-        for (size_t i = 0; i < p.files_in_order.size(); ++i) {
-            const FileInfo &f = p.files_in_order[i];
-            bool touched = false;
-            for (uint64_t b = 0; b < nblk[i] && !touched; ++b)
-                touched = dset.count(first[i] + b) > 0;
-            if (!touched)
-                continue;
-            std::vector<uint8_t> bytes(f.length);
-            if (f.length)
-                detail::cuda_check(cudaMemcpy(bytes.data(), dev.slice(first[i]), f.length, cudaMemcpyDeviceToHost),
-                                   "cudaMemcpy (repaired file)");
-            detail::write_file(dir_ / f.name, bytes.data(), bytes.size());
+        stats_.ms_gpu += ms_since(t3);
+        // write every touched file to <name>.par2tmp, then commit them all
+        const auto t4 = std::chrono::steady_clock::now();
+        std::vector<std::pair<std::filesystem::path, std::filesystem::path>> commits;
+        try {
+            for (size_t i = 0; i < p.files_in_order.size(); ++i) {
+                const FileInfo &f = p.files_in_order[i];
+                bool touched = false;
+                for (uint64_t b = 0; b < nblk[i] && !touched; ++b)
+                    touched = dset.count(first[i] + b) > 0;
+                if (!touched)
+                    continue;
+                check_cancel();
+                std::vector<uint8_t> bytes(f.length);
+                if (f.length)
+                    detail::cuda_check(cudaMemcpy(bytes.data(), dev.slice(first[i]), f.length,
+                                                  cudaMemcpyDeviceToHost),
+                                       "cudaMemcpy (repaired file)");
+                const std::filesystem::path fin = dir_ / f.name;
+                std::filesystem::path tmp = fin;
+                tmp += ".par2tmp";
+                commits.emplace_back(tmp, fin);
+                detail::write_file(tmp, bytes.data(), bytes.size());
+            }
+            check_cancel();
+        } catch (...) {
+            for (const auto &c : commits) {
+                std::error_code ec;
+                std::filesystem::remove(c.first, ec);
+            }
+            throw;
+        }
+        for (const auto &c : commits) {
+            std::filesystem::rename(c.first, c.second);
             ++stats_.files_written;
         }
-        stats_.ms_write = ms_since(t3);
-        stats_.ms_total = ms_since(t0);
+        report(Par2Operation::Repairing, 100, 100);
+        stats_.ms_write = ms_since(t4);
+        finish(p, t0);
         return m;
     }
 
   private:
+    void check_cancel() const
+    {
+        if (cancel_ && cancel_())
+            throw Cancelled();
+    }
+    void report(Par2Operation op, uint64_t cur, uint64_t total) const
+    {
+        if (progress_)
+            progress_(op, cur, total);
+    }
+    // cancellation after the commit skips the purge (lib.rs:338-347)
+    void finish(const Par2File &p, std::chrono::steady_clock::time_point t0)
+    {
+        check_cancel();
+        if (purge_)
+            for (const auto &f : p.set_files) {
+                std::error_code ec;
+                std::filesystem::remove(f, ec);
+            }
+        stats_.ms_total = detail::ms_since(t0);
+    }
+
     std::filesystem::path par2_, dir_;
+    bool do_repair_ = true, purge_ = false;
+    ProgressCallback progress_;
+    detail::CancelFn cancel_;
     PipelineStats stats_;
 };
 

@@ -6,7 +6,10 @@ import os
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "lib",
                         "libpar2format.so")
-OK, ERROR, ESINGULAR, EINSUFFICIENT = 0, -1, -4, -8
+OK, ERROR, ESINGULAR, EINSUFFICIENT, ECANCELLED, EDAMAGED = 0, -1, -4, -8, -9, -10
+OP_SCANNING, OP_LOADING, OP_VERIFYING, OP_REPAIRING = 0, 1, 2, 3
+PROGRESS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64,
+                               ctypes.c_uint64)
 SCHEME_SINGLE, SCHEME_EXPONENTIAL = 0, 1
 
 
@@ -27,6 +30,9 @@ SIGNATURES = [
                     ctypes.c_uint64, ctypes.c_float, ctypes.c_int, ctypes.POINTER(Stats)]),
     ("p2f_repair", [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64),
                     ctypes.POINTER(Stats)]),
+    ("p2f_repair_ex", [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, PROGRESS_FN,
+                       ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                       ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Stats)]),
     ("p2f_last_error", []),
 ]
 
@@ -75,4 +81,19 @@ def repair(par2_path, directory):
     st = Stats()
     _check(lib().p2f_repair(os.fsencode(str(par2_path)), os.fsencode(str(directory)),
                             ctypes.byref(n), ctypes.byref(st)))
+    return n.value, st
+
+
+def repair_ex(par2_path, directory, do_repair=True, purge=False, progress=None, cancel=None):
+    """repair_with_callbacks_cancellable: progress(operation, current, total)
+    is called on this thread; `cancel` is a ctypes.c_int32 another thread may
+    set non-zero.  Returns (slices rebuilt, Stats)."""
+    cb = PROGRESS_FN(lambda user, op, cur, tot: progress(op, cur, tot)) if progress \
+        else PROGRESS_FN()
+    n = ctypes.c_uint64()
+    st = Stats()
+    _check(lib().p2f_repair_ex(os.fsencode(str(par2_path)), os.fsencode(str(directory)),
+                               int(bool(do_repair)), int(bool(purge)), cb, None,
+                               ctypes.byref(cancel) if cancel is not None else None,
+                               ctypes.byref(n), ctypes.byref(st)))
     return n.value, st

@@ -70,3 +70,86 @@ def test_insufficient_recovery(tmp_path):
     with pytest.raises(fmt.Par2FormatError) as ei:
         fmt.repair(tmp_path / "s.par2", tmp_path)
     assert ei.value.code == fmt.EINSUFFICIENT
+
+
+def test_cancel_before_start(tmp_path):
+    import ctypes
+
+    flag = ctypes.c_int32(1)
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair_ex(tmp_path / "none.par2", tmp_path, cancel=flag)
+    assert ei.value.code == fmt.ECANCELLED and "cancelled" in str(ei.value)
+
+
+def _damaged_set(tmp_path, seed):
+    files = make_files(tmp_path, [300000, 1 << 20, 123457], seed)
+    orig = {p.name: p.read_bytes() for p in files}
+    fmt.create(files, tmp_path / "set.par2", block_size=65536, redundancy=50,
+               scheme=fmt.SCHEME_EXPONENTIAL)
+    b = bytearray(orig["part1.bin"])
+    b[70000] ^= 0xFF
+    (tmp_path / "part1.bin").write_bytes(bytes(b))
+    os.unlink(tmp_path / "part2.bin")
+    return files, orig
+
+
+@pytest.mark.gpu
+def test_repair_ex_verify_only_progress_and_purge(tmp_path):
+    files, orig = _damaged_set(tmp_path, 31)
+    seen = []
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair_ex(tmp_path / "set.par2", tmp_path, do_repair=False,
+                      progress=lambda op, c, t: seen.append((op, c, t)))
+    assert ei.value.code == fmt.EDAMAGED
+    assert "repair was not requested" in str(ei.value)
+    assert (fmt.OP_LOADING, 0, 100) in seen and (fmt.OP_VERIFYING, 100, 100) in seen
+    assert (tmp_path / "part1.bin").read_bytes() != orig["part1.bin"]   # untouched
+    seen.clear()
+    par2s = sorted(p.name for p in tmp_path.iterdir() if p.suffix == ".par2")
+    assert len(par2s) > 1
+    n, st = fmt.repair_ex(tmp_path / "set.par2", tmp_path, purge=True,
+                          progress=lambda op, c, t: seen.append((op, c, t)))
+    assert n == 1 + 2 and st.files_written == 2
+    assert (fmt.OP_REPAIRING, 100, 100) in seen
+    for p in files:
+        assert p.read_bytes() == orig[p.name]
+    assert not [p for p in tmp_path.iterdir() if p.suffix in (".par2", ".par2tmp")]
+
+
+@pytest.mark.gpu
+def test_cancel_during_repair_leaves_files_unchanged(tmp_path):
+    import ctypes
+
+    files, orig = _damaged_set(tmp_path, 32)
+    before = {p.name: p.read_bytes() for p in tmp_path.iterdir() if p.suffix == ".bin"}
+    flag = ctypes.c_int32(0)
+
+    def progress(op, cur, tot):
+        if op == fmt.OP_REPAIRING and cur == 0:
+            flag.value = 1
+
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair_ex(tmp_path / "set.par2", tmp_path, progress=progress, cancel=flag)
+    assert ei.value.code == fmt.ECANCELLED
+    after = {p.name: p.read_bytes() for p in tmp_path.iterdir() if p.suffix == ".bin"}
+    assert after == before                       # nothing committed, nothing half-written
+    assert not [p for p in tmp_path.iterdir() if p.suffix == ".par2tmp"]
+
+
+@pytest.mark.gpu
+def test_cancel_after_commit_skips_purge(tmp_path):
+    import ctypes
+
+    files, orig = _damaged_set(tmp_path, 33)
+    flag = ctypes.c_int32(0)
+
+    def progress(op, cur, tot):
+        if op == fmt.OP_REPAIRING and cur == 100:
+            flag.value = 1
+
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair_ex(tmp_path / "set.par2", tmp_path, purge=True, progress=progress, cancel=flag)
+    assert ei.value.code == fmt.ECANCELLED
+    for p in files:                               # the repair was committed
+        assert p.read_bytes() == orig[p.name]
+    assert (tmp_path / "set.par2").exists()       # but the purge was skipped
