@@ -38,6 +38,7 @@ extern "C" {
 #define P2G_ETIMEOUT (-5)   /* a bounded device wait gave up */
 #define P2G_ENODEV (-6)     /* no usable sm_100 device */
 #define P2G_ERANGE (-7)     /* a size beyond a documented maximum */
+#define P2G_ECANCELED (-8)  /* the batch was cancelled (p2g_batch_cancel) */
 
 /* flags */
 #define P2G_DEVICE_PTRS 0x1u /* slice pointers are device pointers */
@@ -234,6 +235,15 @@ int p2g_batch_run(p2g_batch *batch);
 int p2g_batch_launch(p2g_batch *batch);
 int p2g_batch_poll(p2g_batch *batch, int *done);
 int p2g_batch_wait(p2g_batch *batch);
+/* Cancels a launched batch from any thread: a copy engine raises a device
+ * word that the persistent kernels poll, so they take no further work items
+ * (those running finish; nothing waits), and p2g_batch_wait returns
+ * P2G_ECANCELED with every job's status P2G_ECANCELED and its outputs
+ * unspecified (a cancel that lands before the batch starts may let it run to
+ * the end; it is reported cancelled all the same).  The context stays usable;
+ * the next p2g_batch_launch clears the word.  No counterpart in par2-rs (its
+ * Cancelled error, error.rs:34-35, stops host loops between chunks). */
+int p2g_batch_cancel(p2g_batch *batch);
 int p2g_batch_destroy(p2g_batch *batch);
 
 /* Size of the fixed device scratch array behind p2g_encode_noalloc. */

@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <vector>
 
@@ -69,6 +70,9 @@ struct p2g_batch {
     std::vector<HashGroup> hash;
     size_t hash_bytes = 0;  // MD5 + CRC results of all groups
     DevBuf hash_host;  // pinned
+    DevBuf abort_buf;  // device word the persistent kernels poll (p2g_batch_cancel)
+    int *abort_dev = nullptr;
+    std::atomic<bool> cancelled{false};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done = nullptr;
@@ -135,8 +139,8 @@ void batch_free(p2g_batch *b)
         cudaGraphDestroy(b->graph);
     if (b->done)
         cudaEventDestroy(b->done);
-    DevBuf *bufs[] = {&b->params, &b->hparams, &b->planes, &b->recs, &b->rhs,
-                      &b->inv,    &b->hashbuf, &b->hash_host};
+    DevBuf *bufs[] = {&b->params, &b->hparams, &b->planes,    &b->recs,     &b->rhs,
+                      &b->inv,    &b->hashbuf, &b->hash_host, &b->abort_buf};
     for (DevBuf *d : bufs) {
         if (b->ctx)
             give(b->ctx, *d);
@@ -151,6 +155,7 @@ int enqueue(p2g_batch *b)
     p2g_ctx *ctx = b->ctx;
     cudaStream_t st = ctx->stream;
     P2G_CUDA(cudaMemsetAsync(dp(b, b->counter_off), 0, 2 * sizeof(int), st));
+    P2G_CUDA(cudaMemsetAsync(b->abort_dev, 0, sizeof(int), st));
     P2G_TRY(batch_copy(st, reinterpret_cast<const uint8_t *const *>(dp(b, b->copy_src_off)),
                        reinterpret_cast<uint8_t *const *>(dp(b, b->copy_dst_off)),
                        reinterpret_cast<const unsigned long long *>(dp(b, b->copy_len_off)),
@@ -172,7 +177,7 @@ int enqueue(p2g_batch *b)
             ctx->mark(2);
         P2G_TRY(batch_muladd(st, P.grid, reinterpret_cast<const BatchProb *>(dp(b, P.prob_off)),
                              reinterpret_cast<const BatchItem *>(dp(b, P.item_off)), P.nitems,
-                             reinterpret_cast<int *>(dp(b, b->counter_off)) + x));
+                             reinterpret_cast<int *>(dp(b, b->counter_off)) + x, b->abort_dev));
         ctx->launches += 4;
     }
     ctx->mark(3);
@@ -271,6 +276,10 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
         batch_free(b);
         return rc;
     };
+    // the abort word (device memory), cleared by every launch
+    if (int rc = take(ctx, b->abort_buf, 64))
+        return fail(rc);
+    b->abort_dev = b->abort_buf.as<int>();
     // ---- decode matrices of REPAIR jobs ----
     std::vector<size_t> inv_off(njobs, 0);
     size_t inv_bytes = 0;
@@ -695,6 +704,10 @@ int p2g_batch_launch(p2g_batch *b)
     for (bool &m : ctx->ev_marked)
         m = false;
     ctx->mark(0);
+    b->cancelled = false;
+    for (size_t j = 0; j < b->njobs; ++j)  // a cancelled run's statuses (singular jobs keep theirs)
+        if (b->jobs[j].status == P2G_ECANCELED)
+            b->jobs[j].status = P2G_OK;
     if (b->exec) {
         P2G_CUDA(cudaGraphLaunch(b->exec, ctx->stream));
         ctx->launches = 1;
@@ -740,6 +753,12 @@ int p2g_batch_wait(p2g_batch *b)
     P2G_CUDA(cudaEventSynchronize(b->done));
     P2G_CUDA(cudaGetLastError());
     b->launched = false;
+    if (b->cancelled) {
+        for (size_t j = 0; j < b->njobs; ++j)
+            b->jobs[j].status = P2G_ECANCELED;
+        set_error("p2g_batch_wait: batch cancelled");
+        return P2G_ECANCELED;
+    }
     {
         std::lock_guard<std::mutex> lock(ctx->mu);
         ctx->last = p2g_timing{};
@@ -772,6 +791,29 @@ int p2g_batch_run(p2g_batch *b)
 {
     P2G_TRY(p2g_batch_launch(b));
     return p2g_batch_wait(b);
+}
+
+int p2g_batch_cancel(p2g_batch *b)
+{
+    clear_error();
+    if (!b || !b->abort_dev) {
+        set_error("p2g_batch_cancel: null batch");
+        return P2G_EINVAL;
+    }
+    p2g_ctx *ctx = b->ctx;
+    // a copy engine writes the word while the persistent kernel occupies the
+    // SMs (a memset kernel could not start before it ends)
+    static const int one = 1;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        P2G_CUDA(cudaSetDevice(ctx->device));
+        if (!ctx->cancel_stream)
+            P2G_CUDA(cudaStreamCreateWithFlags(&ctx->cancel_stream, cudaStreamNonBlocking));
+        P2G_CUDA(cudaMemcpyAsync(b->abort_dev, &one, sizeof one, cudaMemcpyHostToDevice,
+                                 ctx->cancel_stream));
+    }
+    b->cancelled = true;
+    return P2G_OK;
 }
 
 int p2g_batch_destroy(p2g_batch *b)

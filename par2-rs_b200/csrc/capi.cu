@@ -399,6 +399,10 @@ int p2g_destroy(p2g_ctx *ctx)
         cudaStreamSynchronize(ctx->copy_stream);
         cudaStreamDestroy(ctx->copy_stream);
     }
+    if (ctx->cancel_stream) {
+        cudaStreamSynchronize(ctx->cancel_stream);
+        cudaStreamDestroy(ctx->cancel_stream);
+    }
     if (ctx->own_stream)
         cudaStreamDestroy(ctx->own_stream);
     delete ctx;

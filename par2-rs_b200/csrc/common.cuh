@@ -58,6 +58,8 @@ struct p2g_ctx {
     cudaStream_t stream = nullptr;      // where work runs (own or caller's)
     // host-to-device copies that overlap the kernels (p2g_encode from host)
     cudaStream_t copy_stream = nullptr;
+    // the copy that raises a running batch's abort word (p2g_batch_cancel)
+    cudaStream_t cancel_stream = nullptr;
     static constexpr int kPipe = 16;
     cudaEvent_t pipe_ev[kPipe] = {};
     std::mutex mu;

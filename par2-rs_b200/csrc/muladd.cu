@@ -408,17 +408,23 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
 template <int WARPS, int EREG, int PSPLIT>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     muladd_persistent(const BatchProb *__restrict__ probs, const BatchItem *__restrict__ items,
-                      int nitems, int *__restrict__ counter)
+                      int nitems, int *__restrict__ counter, const volatile int *abort)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ int cur;
+    int stop = 0, fetches = 0;  // the abort flag as read during an earlier item
     while (true) {
+        // a raised abort flag stops the CTA before its next item
         if (threadIdx.x == 0)
-            cur = atomicAdd(counter, 1);
+            cur = stop ? nitems : atomicAdd(counter, 1);
         __syncthreads();
         const int it = cur;
         if (it >= nitems)
             break;
+        // poll the flag on every 4th item, used at a later fetch so that the
+        // read overlaps the item's work
+        if (threadIdx.x == 0 && (fetches++ & 3) == 0)
+            stop = *abort;
         const BatchItem item = items[it];
         const BatchProb p = probs[item.prob];
         const int i0 = static_cast<int>(static_cast<long long>(p.nin) * item.split / p.nsplit);
@@ -914,7 +920,7 @@ int batch_copy(cudaStream_t st, const uint8_t *const *src, uint8_t *const *dst,
 }
 
 int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchItem *items,
-                 int nitems, int *counter)
+                 int nitems, int *counter, const volatile int *abort)
 {
     if (nitems <= 0)
         return P2G_OK;
@@ -926,7 +932,7 @@ int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchI
     auto fn = muladd_persistent<W, E, 1>;
     P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
-    fn<<<grid, W * 32, smem, st>>>(probs, items, nitems, counter);
+    fn<<<grid, W * 32, smem, st>>>(probs, items, nitems, counter, abort);
     P2G_CUDA(cudaGetLastError());
     return P2G_OK;
 }

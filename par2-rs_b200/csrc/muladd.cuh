@@ -46,9 +46,10 @@ int batch_zero(cudaStream_t st, uint8_t *const *ptrs, const unsigned long long *
 int batch_copy(cudaStream_t st, const uint8_t *const *src, uint8_t *const *dst,
                const unsigned long long *bytes, int n);
 // The persistent kernel over `nitems` items (longest first) with `grid` CTAs;
-// *counter must be zero.
+// *counter must be zero.  A CTA takes no further item once it has seen the
+// device word *abort non-zero (polled every 4th item).
 int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchItem *items,
-                 int nitems, int *counter);
+                 int nitems, int *counter, const volatile int *abort);
 
 // The plan for a problem: the context's tuned plan for this shape if there
 // is one, else a heuristic (8 warps, as many outputs per warp as fit).

@@ -23,11 +23,12 @@ ESINGULAR = -4
 ETIMEOUT = -5
 ENODEV = -6
 ERANGE = -7
+ECANCELED = -8
 DEVICE_PTRS = 0x1
 PRIORITY_OPTIMAL = 40
 
 _CODES = {EINVAL: "EINVAL", ENOMEM: "ENOMEM", ECUDA: "ECUDA", ESINGULAR: "ESINGULAR",
-          ETIMEOUT: "ETIMEOUT", ENODEV: "ENODEV", ERANGE: "ERANGE"}
+          ETIMEOUT: "ETIMEOUT", ENODEV: "ENODEV", ERANGE: "ERANGE", ECANCELED: "ECANCELED"}
 
 # (name, restype, argtypes) of every exported entry point
 _P = ctypes.c_void_p
@@ -61,6 +62,7 @@ SIGNATURES = [
     ("p2g_batch_launch", _I, [_P]),
     ("p2g_batch_poll", _I, [_P, _P]),
     ("p2g_batch_wait", _I, [_P]),
+    ("p2g_batch_cancel", _I, [_P]),
     ("p2g_batch_destroy", _I, [_P]),
 ]
 JOB_CREATE, JOB_REPAIR, JOB_VERIFY = 1, 2, 3
@@ -394,6 +396,11 @@ class Batch:
 
     def statuses(self):
         return [self.jobs[j].status for j in range(len(self.specs))]
+
+    def cancel(self):
+        """Stops a launched batch at its next work item (wait() then raises
+        Par2GpuError with code ECANCELED)."""
+        check(lib().p2g_batch_cancel(self.h))
 
     def close(self):
         if getattr(self, "h", None):

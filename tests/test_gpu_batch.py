@@ -158,3 +158,46 @@ def test_unaligned_pointers_rejected(ctx):
     with pytest.raises(par2gpu.Par2GpuError) as ei:
         par2gpu.Batch(ctx, [job])
     assert ei.value.code == par2gpu.EINVAL
+
+
+def test_cancel_stops_the_batch_and_the_context_stays_usable(ctx):
+    """p2g_batch_cancel while the persistent kernel runs: it takes no further
+    item, the batch ends early with P2G_ECANCELED, and the same context then
+    runs a batch correctly."""
+    import time
+
+    import torch
+
+    import par2gpu
+
+    rng = np.random.default_rng(44)
+    k, S, r = 2048, 1 << 20, 205        # ~35 ms of work per job
+    src = torch.randint(0, 256, (k, S), dtype=torch.uint8, device="cuda")
+    outs = [torch.zeros((r, S), dtype=torch.uint8, device="cuda") for _ in range(6)]
+    jobs = [{"kind": par2gpu.JOB_CREATE, "k": k, "slice_bytes": S,
+             "src": [src[i] for i in range(k)], "exps": np.arange(r),
+             "out": [o[e] for e in range(r)]} for o in outs]
+    b = par2gpu.Batch(ctx, jobs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.launch()
+    time.sleep(0.02)
+    b.cancel()
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        b.wait()
+    took = time.perf_counter() - t0
+    assert ei.value.code == par2gpu.ECANCELED
+    assert b.statuses() == [par2gpu.ECANCELED] * len(jobs)
+    assert took < 0.15, took            # well short of the ~210 ms the batch needs
+    # relaunching clears the flag: the full batch completes and is correct
+    assert b.run() == [0] * len(jobs)
+    small = src[:64, :8192].cpu().numpy()
+    want = oracle.encode(small, np.arange(3, dtype=np.uint32))
+    b.close()
+    o = torch.zeros((3, 8192), dtype=torch.uint8, device="cuda")
+    b2 = par2gpu.Batch(ctx, [{"kind": par2gpu.JOB_CREATE, "k": 64, "slice_bytes": 8192,
+                              "src": [src[i] for i in range(64)], "exps": np.arange(3),
+                              "out": [o[e] for e in range(3)]}])
+    assert b2.run() == [0]
+    assert np.array_equal(o.cpu().numpy(), want)
+    b2.close()
