@@ -838,9 +838,24 @@ def serving_pool(dev, nsets, seed):
     return pool
 
 
-def make_jobs(pool, nj, rng, ctx):
+def repair_data(p, ctx):
+    """The recovery slices and erasures of a pool set's repair jobs, made once
+    (its own generator: every job list sees the same data)."""
     import torch
 
+    if "rec" not in p:
+        x = p["spec"]
+        m = max(1, min(x["k"], x.get("m", 1)))
+        prng = np.random.default_rng(x["k"] * 7919 + x["S"])
+        miss = np.sort(prng.choice(x["k"], m, replace=False))
+        rec = torch.zeros((m, x["S"]), dtype=torch.uint8, device=p["src"].device)
+        ctx.encode([p["src"][i] for i in range(x["k"])], x["S"], np.arange(m),
+                   [rec[q] for q in range(m)], device=True)
+        p["rec"], p["miss"] = rec, miss
+    return p["miss"], p["rec"]
+
+
+def make_jobs(pool, nj, rng, ctx):
     from par2gpu.serve import ServedJob
 
     jobs = []
@@ -853,16 +868,8 @@ def make_jobs(pool, nj, rng, ctx):
         elif u < 0.8:
             jobs.append(ServedJob(jid, "verify", p["src"]))
         else:
-            if "rec" not in p:
-                m = max(1, min(x["k"], x.get("m", 1)))
-                # own generator: both job lists must draw the same sequence
-                prng = np.random.default_rng(x["k"] * 7919 + x["S"])
-                miss = np.sort(prng.choice(x["k"], m, replace=False))
-                rec = torch.zeros((m, x["S"]), dtype=torch.uint8, device=p["src"].device)
-                ctx.encode([p["src"][i] for i in range(x["k"])], x["S"], np.arange(m),
-                           [rec[q] for q in range(m)], device=True)
-                p["rec"], p["miss"] = rec, miss
-            jobs.append(ServedJob(jid, "repair", p["src"], missing=p["miss"], rec=p["rec"]))
+            miss, rec = repair_data(p, ctx)
+            jobs.append(ServedJob(jid, "repair", p["src"], missing=miss, rec=rec))
     return jobs
 
 
@@ -880,16 +887,29 @@ def run_serving(args):
     ctxs = [par2gpu.Context(0), par2gpu.Context(0), par2gpu.Context(0)]
     pool = serving_pool(dev, 48, SEED + 21)
     torch.cuda.synchronize(dev)
-    # untimed warm-up of both servers (module loads, first launches, scratch)
+    # untimed warm-up of both servers to their steady state: every set of the
+    # pool as a create, a verify and a repair job, so that every scratch
+    # buffer has reached its size (growing one frees it, and a free
+    # synchronises the device)
+    from par2gpu.serve import ServedJob
+
+    warm = []
+    for p in pool:
+        miss, rec = repair_data(p, ctxs[0])
+        warm.append(ServedJob(len(warm), "create", p["src"], r=p["spec"]["r"]))
+        warm.append(ServedJob(len(warm), "verify", p["src"]))
+        warm.append(ServedJob(len(warm), "repair", p["src"], missing=miss, rec=rec))
     for _ in range(2):
-        warm = make_jobs(pool, 16, np.random.default_rng(SEED + 7), ctxs[0])
+        for j in warm:
+            j.out = j.md5 = j.crc = j.inverse = None
         serve_continuous(ctxs, warm, np.zeros(len(warm)))
         serve_one_at_a_time(ctxs[0], warm, np.zeros(len(warm)))
+    del warm
     torch.cuda.synchronize(dev)
     results = []
     for lam in (10, 100, 500, 1000, 2000):
         rng = np.random.default_rng(SEED + lam)
-        nj = int(min(240, max(40, lam * 1.5)))
+        nj = int(min(240, max(120, lam * 1.5)))
         arrivals = np.cumsum(rng.exponential(1.0 / lam, nj))
         jobs_a = make_jobs(pool, nj, np.random.default_rng(SEED + 100 + lam), ctxs[0])
         jobs_b = make_jobs(pool, nj, np.random.default_rng(SEED + 100 + lam), ctxs[0])

@@ -150,10 +150,14 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
     def build(ctx):
         """Pick units round-robin from admitted jobs up to the iteration
         budget, then merge each job's contiguous units into one spec so that
-        its coefficient records are built once per batch."""
+        its coefficient records are built once per batch.  A job alone with
+        nothing queued gets 16 budgets: cutting it finer only rebuilds its
+        records, and a job that arrives meanwhile waits for at most that."""
         picked, work = [], 0.0
+        alone = sum(1 for e in active if e[1]) == 1 and not queue
+        budget = iter_macs * (16 if alone else 1)
         progress = True
-        while progress and work < iter_macs:
+        while progress and work < budget:
             progress = False
             for _ in range(len(active)):
                 ent = active[0]
@@ -165,7 +169,7 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
                 picked.append((job, u))
                 work += _unit_work(job, u)
                 progress = True
-                if work >= iter_macs:
+                if work >= budget:
                     break
         if not picked:
             return None
