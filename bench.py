@@ -263,10 +263,10 @@ def run_ours(args, rank, world):
         return
 
     # ---- end to end through the C ABI with pinned host buffers (e2e) ----
-    src_h = src_pinned.numpy()
-    out_h = out_pinned.numpy()
-    host_src = [src_h[i] for i in range(k)]
-    host_out = [out_h[e] for e in range(r)]
+    # [k, S] / [r, S] host arrays: the binding passes one pointer per row
+    # (base + i * stride), as a C caller passes its slice table
+    host_src = src_pinned.numpy()
+    host_out = out_pinned.numpy()
     e2e_steps = max(1, args.steps)
     ctx.encode(host_src, S, exps, host_out)  # warm the staging buffers
     barrier()

@@ -5,6 +5,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "common.cuh"
@@ -114,7 +115,10 @@ static int upload_params(p2g_ctx *ctx, const ParamLayout &L)
     return P2G_OK;
 }
 
-constexpr int kTailSlabs = 4;  // column slabs of the last input group (host outputs)
+constexpr int kTailGroups = 2;     // input groups processed slab by slab (host outputs)
+constexpr int kMaxTailSlabs = 16;  // column slabs of those groups, at most
+constexpr int kSlabEvents = p2g_ctx::kPipe;  // pipe_ev index of the first slab event
+static_assert(kSlabEvents + 2 * kMaxTailSlabs + 1 <= p2g_ctx::kPipeEvents, "slab events");
 
 static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
@@ -315,7 +319,8 @@ int p2g_create(int device, p2g_ctx **out)
             break;
         }
         ctx->stream = ctx->own_stream;
-        if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking) != cudaSuccess) {
             set_error("cudaStreamCreate failed");
             rc = P2G_ECUDA;
             break;
@@ -398,6 +403,10 @@ int p2g_destroy(p2g_ctx *ctx)
     if (ctx->copy_stream) {
         cudaStreamSynchronize(ctx->copy_stream);
         cudaStreamDestroy(ctx->copy_stream);
+    }
+    if (ctx->d2h_stream) {
+        cudaStreamSynchronize(ctx->d2h_stream);
+        cudaStreamDestroy(ctx->d2h_stream);
     }
     if (ctx->cancel_stream) {
         cudaStreamSynchronize(ctx->cancel_stream);
@@ -537,15 +546,28 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     bool s_staged = false, d_staged = false;
     P2G_TRY(stage(ctx, ctx->in_copy, src, k, slice_bytes, dev, groups == 1, s, s_staged));
     P2G_TRY(stage(ctx, ctx->out_copy, out, r, slice_bytes, dev, false, d, d_staged));
-    // With host outputs, the last input group runs as column slabs: the
-    // outputs of a finished slab go back while the next slab computes.
+    // With host outputs, the last kTailGroups input groups run slab by slab
+    // (column ranges): a slab's inputs go up, its outputs are then final and
+    // go back on their own stream while the next slab goes up -- both PCIe
+    // directions busy -- instead of reading all outputs back after the end.
+    // Slabs are sized to whole waves: one slab's launch (slab tiles x output
+    // blocks CTAs) about fills the device, so none leaves SMs idle.
     const size_t tiles = (slice_bytes + 2047) / 2048;
-    const int slabs = (groups > 1 && d_staged && tiles >= 32) ? kTailSlabs : 1;
-    const size_t last0 = k * (groups - 1) / groups, nlast = k - last0;
+    int slabs = 1;
+    if (groups >= 4 && d_staged) {
+        const p2g::MuladdPlan tp = p2g::choose_plan(ctx, static_cast<int>(k / groups * kTailGroups),
+                                                    static_cast<int>(r), slice_bytes);
+        const double waves = static_cast<double>(tiles) * tp.nblk / p2g::plan_slots(ctx, tp);
+        slabs = static_cast<int>(std::min<double>(kMaxTailSlabs, std::floor(waves + 0.5)));
+        if (static_cast<size_t>(slabs) > tiles)
+            slabs = 1;
+    }
+    const bool tail = slabs >= 2;
+    const size_t t0 = tail ? k * (groups - kTailGroups) / groups : k, ntail = k - t0;
     std::vector<size_t> cut(slabs + 1);
     for (int q = 0; q <= slabs; ++q)
         cut[q] = q == slabs ? slice_bytes : tiles * q / slabs * 2048;
-    const size_t tail_bytes = slabs > 1 ? slabs * (nlast + r) * sizeof(void *) : 0;
+    const size_t tail_bytes = tail ? slabs * (ntail + r) * sizeof(void *) : 0;
     ParamLayout L(k, r, k * 2, round16(r * 4) + tail_bytes);
     P2G_TRY(ctx->hparams.ensure(L.total));
     P2G_TRY(ctx->params.ensure(L.total));
@@ -555,15 +577,22 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     par2_constants(k, reinterpret_cast<uint16_t *>(h + L.a_off));
     memcpy(h + L.b_off, exps, r * 4);
     const size_t tail_off = L.b_off + round16(r * 4);
-    if (slabs > 1) {
-        // per slab: the last group's inputs, then the outputs, offset to the slab
+    if (tail) {
+        // per slab: the tail inputs, then the outputs, offset to the slab
         uint8_t **t = reinterpret_cast<uint8_t **>(h + tail_off);
         for (int q = 0; q < slabs; ++q) {
-            for (size_t i = 0; i < nlast; ++i)
-                *t++ = s[last0 + i] + cut[q];
+            for (size_t i = 0; i < ntail; ++i)
+                *t++ = s[t0 + i] + cut[q];
             for (size_t e = 0; e < r; ++e)
                 *t++ = d[e] + cut[q];
         }
+    }
+    // the copy stream starts after everything already queued on the compute
+    // stream (earlier users of the staging buffers), not after this call's
+    // records
+    if (groups > 1) {
+        P2G_CUDA(cudaEventRecord(ctx->pipe_ev[0], ctx->stream));
+        P2G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ev[0], 0));
     }
     P2G_TRY(upload_params(ctx, L));
     uint8_t *dp = ctx->params.as<uint8_t>();
@@ -577,46 +606,50 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
         P2G_TRY(muladd_run(ctx, d_src, static_cast<int>(k), d_dst, static_cast<int>(r),
                            slice_bytes, ctx->recs.as<uint32_t>(), 0));
     } else {
-        // the copy stream starts after everything already queued on the
-        // compute stream (earlier users of the staging buffers)
-        P2G_CUDA(cudaEventRecord(ctx->pipe_ev[0], ctx->stream));
-        P2G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ev[0], 0));
-        for (int g = 0; g < groups; ++g) {
+        const int full = tail ? groups - kTailGroups : groups;
+        for (int g = 0; g < full; ++g) {
             const size_t i0 = k * g / groups, i1 = k * (g + 1) / groups;
             P2G_TRY(copy_slices(s.data() + i0, src + i0, i1 - i0, slice_bytes,
                                 cudaMemcpyHostToDevice, ctx->copy_stream));
             P2G_CUDA(cudaEventRecord(ctx->pipe_ev[g], ctx->copy_stream));
             P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
-            if (g < groups - 1 || slabs == 1) {
-                P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
-                                   static_cast<int>(r), slice_bytes,
-                                   ctx->recs.as<uint32_t>() + i0 * r * 16, g == 0 ? 0 : 1));
-                continue;
-            }
-            // the last group, slab by slab; each slab's outputs go back on the
-            // copy stream (its uploads are done) as soon as the slab is final
+            P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
+                               static_cast<int>(r), slice_bytes,
+                               ctx->recs.as<uint32_t>() + i0 * r * 16, g == 0 ? 0 : 1));
+        }
+        if (tail) {
             uint8_t *const *tab = reinterpret_cast<uint8_t *const *>(dp + tail_off);
-            std::vector<uint8_t *> uo(r), so(r);
+            std::vector<const uint8_t *> hs(ntail);
+            std::vector<uint8_t *> ds(ntail), uo(r), so(r);
+            cudaEvent_t *up = ctx->pipe_ev + kSlabEvents, *done = up + slabs;
             for (int q = 0; q < slabs; ++q) {
-                const uint8_t *const *qs = reinterpret_cast<const uint8_t *const *>(tab + q * (nlast + r));
-                P2G_TRY(muladd_run(ctx, qs, static_cast<int>(nlast), tab + q * (nlast + r) + nlast,
-                                   static_cast<int>(r), cut[q + 1] - cut[q],
-                                   ctx->recs.as<uint32_t>() + i0 * r * 16, 1));
-                P2G_CUDA(cudaEventRecord(ctx->pipe_ev[q], ctx->stream));
-                P2G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ev[q], 0));
+                const size_t w = cut[q + 1] - cut[q];
+                for (size_t i = 0; i < ntail; ++i) {
+                    hs[i] = src[t0 + i] + cut[q];
+                    ds[i] = s[t0 + i] + cut[q];
+                }
+                P2G_TRY(copy_slices(ds.data(), hs.data(), ntail, w, cudaMemcpyHostToDevice,
+                                    ctx->copy_stream));
+                P2G_CUDA(cudaEventRecord(up[q], ctx->copy_stream));
+                P2G_CUDA(cudaStreamWaitEvent(ctx->stream, up[q], 0));
+                const uint8_t *const *qs = reinterpret_cast<const uint8_t *const *>(tab + q * (ntail + r));
+                P2G_TRY(muladd_run(ctx, qs, static_cast<int>(ntail), tab + q * (ntail + r) + ntail,
+                                   static_cast<int>(r), w, ctx->recs.as<uint32_t>() + t0 * r * 16, 1));
+                P2G_CUDA(cudaEventRecord(done[q], ctx->stream));
+                P2G_CUDA(cudaStreamWaitEvent(ctx->d2h_stream, done[q], 0));
                 for (size_t e = 0; e < r; ++e) {
                     uo[e] = out[e] + cut[q];
                     so[e] = d[e] + cut[q];
                 }
-                P2G_TRY(copy_slices(uo.data(), so.data(), r, cut[q + 1] - cut[q],
-                                    cudaMemcpyDeviceToHost, ctx->copy_stream));
+                P2G_TRY(copy_slices(uo.data(), so.data(), r, w, cudaMemcpyDeviceToHost,
+                                    ctx->d2h_stream));
             }
             // the call ends when the last read-back has landed
-            P2G_CUDA(cudaEventRecord(ctx->pipe_ev[slabs], ctx->copy_stream));
-            P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[slabs], 0));
+            P2G_CUDA(cudaEventRecord(done[slabs], ctx->d2h_stream));
+            P2G_CUDA(cudaStreamWaitEvent(ctx->stream, done[slabs], 0));
         }
     }
-    if (d_staged && slabs == 1)
+    if (d_staged && !tail)
         P2G_TRY(unstage(ctx, out, d, r, slice_bytes, dev));
     return finish(ctx);
 }

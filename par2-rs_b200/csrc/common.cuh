@@ -58,10 +58,13 @@ struct p2g_ctx {
     cudaStream_t stream = nullptr;      // where work runs (own or caller's)
     // host-to-device copies that overlap the kernels (p2g_encode from host)
     cudaStream_t copy_stream = nullptr;
+    // device-to-host read-back of finished output slabs (p2g_encode to host)
+    cudaStream_t d2h_stream = nullptr;
     // the copy that raises a running batch's abort word (p2g_batch_cancel)
     cudaStream_t cancel_stream = nullptr;
-    static constexpr int kPipe = 16;
-    cudaEvent_t pipe_ev[kPipe] = {};
+    static constexpr int kPipe = 16;        // input groups of a host encode
+    static constexpr int kPipeEvents = 56;  // group events + slab events
+    cudaEvent_t pipe_ev[kPipeEvents] = {};
     std::mutex mu;
     // optional per-phase timing (p2g_set_timing / p2g_last_timing)
     bool timing = false;

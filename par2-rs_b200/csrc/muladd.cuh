@@ -54,6 +54,8 @@ int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchI
 // The plan for a problem: the context's tuned plan for this shape if there
 // is one, else a heuristic (8 warps, as many outputs per warp as fit).
 MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t slice_bytes);
+// CTAs of plan p the device runs at once (SMs x CTAs resident per SM).
+int plan_slots(const p2g_ctx *ctx, const MuladdPlan &p);
 bool plan_valid(const MuladdPlan &p, int nin, int nout, size_t slice_bytes);
 // The compiled (warps, outputs per group, warps per group) shapes; returns
 // their number.

@@ -167,11 +167,28 @@ def _ptr(x):
 
 def _ptr_array(xs):
     """A C array of pointers: from a numpy uint64 array of addresses (used as
-    is), or from a list of ints / tensors / arrays."""
-    if isinstance(xs, np.ndarray) and xs.dtype == np.uint64:
-        return np.ascontiguousarray(xs) if len(xs) else np.zeros(1, np.uint64)
+    is), from a 2-D array or tensor (one pointer per row, computed from its
+    base and row stride), or from a list of ints / tensors / arrays."""
+    if isinstance(xs, np.ndarray) and xs.dtype == np.uint64 and xs.ndim == 1:
+        return _addr_param(np.ascontiguousarray(xs) if len(xs) else np.zeros(1, np.uint64))
+    if isinstance(xs, np.ndarray) and xs.ndim == 2:
+        return _row_addresses(xs.ctypes.data, xs.strides[0], xs.shape[0])
+    if hasattr(xs, "data_ptr") and xs.dim() == 2:
+        return _row_addresses(xs.data_ptr(), xs.stride(0) * xs.element_size(), xs.shape[0])
     arr = (ctypes.c_void_p * max(1, len(xs)))(*[_ptr(x) for x in xs])
     return arr
+
+
+def _row_addresses(base, stride, n):
+    if n == 0:
+        return _addr_param(np.zeros(1, np.uint64))
+    return _addr_param(np.uint64(base) + np.arange(n, dtype=np.uint64) * np.uint64(stride))
+
+
+def _addr_param(a):
+    # a void* argument over a uint64 address array; the pointer object holds
+    # a reference to the array, so it lives until the call returns
+    return a.ctypes.data_as(ctypes.c_void_p)
 
 
 def _as_voidp(a):
@@ -263,7 +280,7 @@ class Context:
         src = np.ascontiguousarray(src, np.uint8)
         k, S = src.shape
         out = np.zeros((len(exps), S), np.uint8)
-        self.encode([src[i] for i in range(k)], S, exps, [out[e] for e in range(len(exps))])
+        self.encode(src, S, exps, out)
         return out
 
     # --- repair (par2_rs.rs:319-675) --------------------------------------

@@ -75,8 +75,8 @@ def test_encode_matches_oracle(ctx, k, S, r):
 @pytest.mark.parametrize("k,S,r", [(128, 65536, 9), (300, 65536 + 2050, 7), (200, 131072 + 4, 30)])
 def test_host_pipeline_groups_and_tail_slabs(ctx, k, S, r):
     """Host buffers with k >= 128: inputs go up in groups while earlier groups
-    are accumulated, and the last group runs as column slabs whose outputs go
-    back while the next slab computes (ragged last slab included)."""
+    are accumulated (slices this narrow fill under 1.5 waves, so the outputs
+    are read back whole at the end)."""
     rng = np.random.default_rng(k + S)
     src = rng.integers(0, 256, (k, S), dtype=np.uint8)
     exps = np.arange(r, dtype=np.uint32)
@@ -87,6 +87,30 @@ def test_host_pipeline_groups_and_tail_slabs(ctx, k, S, r):
     outs = [np.zeros(S, np.uint8) for _ in range(r)]
     ctx.encode(rows, S, exps, outs)
     assert np.array_equal(np.stack(outs), want)
+
+
+@pytest.mark.parametrize("k,S,r", [(256, (1 << 20) + 6, 205), (320, 600 * 1024 + 2050, 110)])
+def test_host_pipeline_wave_sized_slabs(ctx, k, S, r):
+    """Slices wide enough that the tail runs as several wave-sized column
+    slabs (7 for 1 MiB x 205 outputs, 4 for 600 KiB x 110, ragged last
+    tile): the host pipeline equals the device-resident single launch over
+    the whole width, and the oracle on column windows (encoding is
+    column-independent) at the start, in the middle and at the end."""
+    import torch
+
+    rng = np.random.default_rng(S)
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(r, dtype=np.uint32)
+    got = ctx.encode_array(src, exps)
+    d_src = torch.from_numpy(src).cuda()
+    d_out = torch.zeros((r, S), dtype=torch.uint8, device="cuda")
+    ctx.encode(d_src, S, exps, d_out, device=True)
+    torch.cuda.synchronize()
+    assert np.array_equal(got, d_out.cpu().numpy())
+    tiles = (S + 2047) // 2048
+    cut = tiles // 2 * 2048  # a slab boundary for an even slab count
+    for c0, c1 in ((0, 4096), (cut - 2048, cut + 2048), (S - 4098, S)):
+        assert np.array_equal(got[:, c0:c1], oracle.encode(np.ascontiguousarray(src[:, c0:c1]), exps))
 
 
 def test_encode_sparse_exponents_and_zero_slices(ctx):
