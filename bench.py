@@ -603,23 +603,48 @@ def run_create_files(args):
             p = os.path.join(d, f"file{i}.bin")
             rng.integers(0, 256, fsize, dtype=np.uint8).tofile(p)
             files.append(p)
-        # warm-up on a small set (device context, kernels, reader threads)
-        wp = os.path.join(d, "warm.bin")
-        rng.integers(0, 256, 8 << 20, dtype=np.uint8).tofile(wp)
+        # warm-up on a small set of as many files (device context, kernels,
+        # one reader thread per file, the pooled pinned chunks they use)
+        warm = []
+        for i in range(nfiles):
+            wp = os.path.join(d, f"warm{i}.bin")
+            rng.integers(0, 256, 8 << 20, dtype=np.uint8).tofile(wp)
+            warm.append(wp)
         for _ in range(max(1, args.warmup)):
-            fmt.create([wp], os.path.join(d, "warm.par2"), block_size=bs, redundancy=pct)
+            fmt.create(warm, os.path.join(d, "warm.par2"), block_size=bs, redundancy=pct)
         out = os.path.join(d, "set.par2")
-        st = fmt.create(files, out, block_size=bs, redundancy=pct)
         total = nfiles * fsize
-        # damage: 200 slices of file 1 zeroed
-        with open(files[1], "r+b") as f:
-            f.write(bytes(200 * bs))
-        n, rst = fmt.repair(out, d)
+        steps = max(1, args.steps)
+
+        def phases(st):  # total / ingest / gpu / write ms of one run
+            return [round(v, 1) for v in (st.ms_total, st.ms_ingest, st.ms_gpu, st.ms_write)]
+
+        def median_run(runs):
+            runs = sorted(runs, key=lambda x: x[0].ms_total)
+            return runs[len(runs) // 2]
+
+        creates = []
+        for _ in range(steps):
+            for f in os.listdir(d):
+                if f.startswith("set."):
+                    os.remove(os.path.join(d, f))
+            creates.append((fmt.create(files, out, block_size=bs, redundancy=pct), None))
+        st = median_run(creates)[0]
+        repairs = []
+        for _ in range(steps):
+            # damage: 200 slices of file 1 zeroed
+            with open(files[1], "r+b") as f:
+                f.write(bytes(200 * bs))
+            n, rst_i = fmt.repair(out, d)
+            repairs.append((rst_i, n))
+        rst, n = median_run(repairs)
         res = {"workload": f"create_files: {nfiles} files x {fsize >> 20} MiB (tmpfs: "
                            f"{base is not None}), {bs >> 20} MiB slices, {pct:g}% recovery; repair "
-                           "of 200 zeroed slices",
-               "create": dict(st.as_dict(), gbs=total / (st.ms_total * 1e-3) / 1e9),
-               "repair": dict(rst.as_dict(), rebuilt=n, gbs=total / (rst.ms_total * 1e-3) / 1e9)}
+                           f"of 200 zeroed slices; median of {steps} runs each",
+               "create": dict(st.as_dict(), gbs=total / (st.ms_total * 1e-3) / 1e9,
+                              runs_ms=[phases(x[0]) for x in creates]),
+               "repair": dict(rst.as_dict(), rebuilt=n, gbs=total / (rst.ms_total * 1e-3) / 1e9,
+                              runs_ms=[phases(x[0]) for x in repairs])}
         # the reference's CPU create path (restated; oracle = OpenSSL MD5, zlib CRC32)
         from oracle import oracle
 

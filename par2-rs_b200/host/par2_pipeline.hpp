@@ -14,10 +14,15 @@
 // recovery slices come back to the host.
 #pragma once
 #include <cuda_runtime.h>
+#include <fcntl.h>
+#include <unistd.h>
 
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <functional>
+#include <memory>
+#include <mutex>
 #include <set>
 #include <thread>
 
@@ -89,6 +94,46 @@ class DeviceSlices {
     uint64_t k_, bs_;
 };
 
+// Process-wide pool of pinned 8 MiB host chunks for the pipelines' copies.
+// Pinning is far slower than the copies it serves (tens of ms for the ~100
+// MiB a create uses), so chunks are pinned once, on first demand, and reused
+// by every later ingest and read-back; they live until the process exits.
+constexpr size_t kPinnedChunk = 8u << 20;
+
+class PinnedPool {
+  public:
+    static PinnedPool &get()
+    {
+        static PinnedPool *p = new PinnedPool;  // never destroyed: see above
+        return *p;
+    }
+    uint8_t *take()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (!free_.empty()) {
+                uint8_t *b = free_.back();
+                free_.pop_back();
+                return b;
+            }
+        }
+        void *b = nullptr;
+        cuda_check(cudaMallocHost(&b, kPinnedChunk), "cudaMallocHost");
+        return static_cast<uint8_t *>(b);
+    }
+    void give(uint8_t *b)
+    {
+        if (!b)
+            return;
+        std::lock_guard<std::mutex> lk(mu_);
+        free_.push_back(b);
+    }
+
+  private:
+    std::mutex mu_;
+    std::vector<uint8_t *> free_;
+};
+
 struct IngestJob {
     std::filesystem::path path;
     uint8_t *dst = nullptr;   // device: the file's first slice
@@ -98,27 +143,31 @@ struct IngestJob {
     bool ok = false;          // out: the file existed and had `length` bytes
 };
 
-// Reads every job's file into device memory with whole-file MD5s, `threads`
-// files at a time.
 // true when the caller asked to stop (polled between phases and read chunks)
 using CancelFn = std::function<bool()>;
 
+// Reads every job's file into device memory with whole-file MD5s, `threads`
+// files at a time.  Per file, a read-ahead thread fills a ring of three
+// pinned 8 MiB chunks while the worker folds the previous chunk into the MD5
+// and uploads it on its own stream, so reading, hashing and uploading
+// overlap (a chunk is refilled only after its upload has finished).
 inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads,
                        const CancelFn *cancel = nullptr)
 {
     auto cancelled = [&] { return cancel && *cancel && (*cancel)(); };
-    constexpr size_t kChunk = 8u << 20;
+    constexpr size_t kChunk = kPinnedChunk;
+    constexpr int kSlots = 3;
     std::atomic<size_t> next{0};
     std::atomic<uint64_t> total{0};
     std::vector<std::string> errors(threads);
     auto worker = [&](unsigned t) {
         cudaStream_t st = nullptr;
-        uint8_t *buf[2] = {nullptr, nullptr};
-        cudaEvent_t ev[2] = {nullptr, nullptr};
+        uint8_t *buf[kSlots] = {};
+        cudaEvent_t ev[kSlots] = {};
         try {
             cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
-            for (int b = 0; b < 2; ++b) {
-                cuda_check(cudaMallocHost(reinterpret_cast<void **>(&buf[b]), kChunk), "cudaMallocHost");
+            for (int b = 0; b < kSlots; ++b) {
+                buf[b] = PinnedPool::get().take();
                 cuda_check(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming), "cudaEventCreate");
             }
             for (size_t j; !cancelled() && (j = next.fetch_add(1)) < jobs.size();) {
@@ -126,22 +175,71 @@ inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads,
                 FILE *f = fopen(job.path.string().c_str(), "rb");
                 if (!f)
                     continue;  // missing file: its slices stay zero
+                std::mutex mu;
+                std::condition_variable cv;
+                size_t len[kSlots] = {};
+                bool full[kSlots] = {}, stop = false;
+                std::thread reader([&] {
+                    uint64_t roff = 0;
+                    for (size_t i = 0;; ++i) {
+                        const int s = static_cast<int>(i % kSlots);
+                        {
+                            std::unique_lock<std::mutex> lk(mu);
+                            cv.wait(lk, [&] { return !full[s] || stop; });
+                            if (stop)
+                                return;
+                        }
+                        cudaEventSynchronize(ev[s]);  // the slot's last upload is done
+                        size_t n = 0;
+                        if (roff < job.length && !cancelled())
+                            n = fread(buf[s], 1, std::min<uint64_t>(kChunk, job.length - roff), f);
+                        roff += n;
+                        {
+                            std::lock_guard<std::mutex> lk(mu);
+                            len[s] = n;
+                            full[s] = true;
+                        }
+                        cv.notify_all();
+                        if (n == 0)
+                            return;
+                    }
+                });
                 Md5 h;
                 uint64_t off = 0;
-                int b = 0;
-                while (off < job.length && !cancelled()) {
-                    cuda_check(cudaEventSynchronize(ev[b]), "cudaEventSynchronize");
-                    const size_t n = fread(buf[b], 1, std::min<uint64_t>(kChunk, job.length - off), f);
-                    if (n == 0)
-                        break;
-                    if (job.hash)
-                        h.update(buf[b], n);
-                    cuda_check(cudaMemcpyAsync(job.dst + off, buf[b], n, cudaMemcpyHostToDevice, st),
-                               "cudaMemcpyAsync");
-                    cuda_check(cudaEventRecord(ev[b], st), "cudaEventRecord");
-                    off += n;
-                    b ^= 1;
+                try {
+                    for (size_t i = 0;; ++i) {
+                        const int s = static_cast<int>(i % kSlots);
+                        size_t n;
+                        {
+                            std::unique_lock<std::mutex> lk(mu);
+                            cv.wait(lk, [&] { return full[s]; });
+                            n = len[s];
+                        }
+                        if (n == 0)
+                            break;
+                        if (job.hash)
+                            h.update(buf[s], n);
+                        cuda_check(cudaMemcpyAsync(job.dst + off, buf[s], n, cudaMemcpyHostToDevice, st),
+                                   "cudaMemcpyAsync");
+                        cuda_check(cudaEventRecord(ev[s], st), "cudaEventRecord");
+                        off += n;
+                        {
+                            std::lock_guard<std::mutex> lk(mu);
+                            full[s] = false;
+                        }
+                        cv.notify_all();
+                    }
+                } catch (...) {
+                    {
+                        std::lock_guard<std::mutex> lk(mu);
+                        stop = true;
+                    }
+                    cv.notify_all();
+                    reader.join();
+                    fclose(f);
+                    throw;
                 }
+                reader.join();
                 uint8_t extra;
                 job.ok = off == job.length && fread(&extra, 1, 1, f) == 0;
                 fclose(f);
@@ -152,11 +250,12 @@ inline uint64_t ingest(std::vector<IngestJob> &jobs, unsigned threads,
         } catch (const std::exception &e) {
             errors[t] = e.what();
         }
-        for (int b = 0; b < 2; ++b) {
+        if (st)
+            cudaStreamSynchronize(st);
+        for (int b = 0; b < kSlots; ++b) {
             if (ev[b])
                 cudaEventDestroy(ev[b]);
-            if (buf[b])
-                cudaFreeHost(buf[b]);
+            PinnedPool::get().give(buf[b]);
         }
         if (st)
             cudaStreamDestroy(st);
@@ -190,15 +289,78 @@ inline std::vector<uint8_t> read_head(const std::filesystem::path &p, size_t n)
     return d;
 }
 
-inline void write_file(const std::filesystem::path &p, const uint8_t *d, size_t n)
+// Runs sink(chunk bytes, offset, length) over n bytes of device memory cut
+// into 8 MiB chunks: up to 8 host threads each copy chunks down through their
+// own pooled pinned buffer and stream and hand them to the sink, so the
+// copies and the sinks (file writes, page faults of the destination) run side
+// by side.  Returns false when a copy or a sink failed.
+template <class Sink> bool drain_device(const uint8_t *d, size_t n, Sink sink)
 {
-    FILE *f = fopen(p.string().c_str(), "wb");
-    if (!f || (n && fwrite(d, 1, n, f) != n)) {
-        if (f)
-            fclose(f);
+    constexpr size_t kChunk = kPinnedChunk;
+    const size_t chunks = (n + kChunk - 1) / kChunk;
+    const size_t nt = std::min<size_t>(
+        chunks, std::min(8u, std::max(1u, std::thread::hardware_concurrency())));
+    std::atomic<size_t> next{0};
+    std::atomic<bool> failed{false};
+    auto worker = [&] {
+        uint8_t *buf = nullptr;
+        cudaStream_t st = nullptr;
+        try {
+            buf = PinnedPool::get().take();
+        } catch (const Par2Error &) {
+            failed = true;
+        }
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+            failed = true;
+        for (size_t c; !failed && (c = next.fetch_add(1)) < chunks;) {
+            const size_t off = c * kChunk, len = std::min(kChunk, n - off);
+            if (cudaMemcpyAsync(buf, d + off, len, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess ||
+                !sink(static_cast<const uint8_t *>(buf), off, len))
+                failed = true;
+        }
+        if (st)
+            cudaStreamDestroy(st);
+        PinnedPool::get().give(buf);
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; ++t)
+        pool.emplace_back(worker);
+    for (auto &th : pool)
+        th.join();
+    if (failed)
+        (void)cudaGetLastError();
+    return !failed;
+}
+
+// Copies n bytes of device memory into host memory h (any, pageable).
+inline void copy_to_host(uint8_t *h, const uint8_t *d, size_t n)
+{
+    if (!drain_device(d, n, [&](const uint8_t *b, size_t off, size_t len) {
+            memcpy(h + off, b, len);
+            return true;
+        }))
+        throw Par2Error("cudaMemcpy (device to host) failed");
+}
+
+// Writes n bytes of device memory to a new file at p (pwrite at each chunk's
+// offset).
+inline void write_file_from_device(const std::filesystem::path &p, const uint8_t *d, size_t n)
+{
+    const int fd = ::open(p.string().c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0)
         throw Par2Error("Failed to write " + p.string());
-    }
-    fclose(f);
+    const bool ok = drain_device(d, n, [&](const uint8_t *b, size_t off, size_t len) {
+        for (size_t w = 0; w < len;) {
+            const ssize_t x = ::pwrite(fd, b + w, len - w, static_cast<off_t>(off + w));
+            if (x <= 0)
+                return false;
+            w += static_cast<size_t>(x);
+        }
+        return true;
+    });
+    if (::close(fd) != 0 || !ok)
+        throw Par2Error("Failed to write " + p.string());
 }
 
 // fn(i) for i in [0, n) on the host's threads
@@ -333,7 +495,9 @@ class Par2Creator {
         stats_.ms_ingest = ms_since(t1);
         // IFSC checksums and recovery slices from the device-resident slices
         const auto t2 = std::chrono::steady_clock::now();
-        std::vector<uint8_t> md5(k * 16), rec(static_cast<size_t>(r * bs));
+        std::vector<uint8_t> md5(k * 16);
+        // filled by the copy below (not zero-initialised first)
+        std::unique_ptr<uint8_t[]> rec(new uint8_t[static_cast<size_t>(r * bs)]);
         std::vector<uint32_t> crc(k);
         if (k) {
             std::vector<const uint8_t *> sp = dev.ptrs(0, k);
@@ -349,8 +513,7 @@ class Par2Creator {
                 }
                 check(p2g_encode(codec_ctx(), sp.data(), k, bs, exps.data(), r, op.data(),
                                  P2G_DEVICE_PTRS));
-                detail::cuda_check(cudaMemcpy(rec.data(), out.slice(0), r * bs, cudaMemcpyDeviceToHost),
-                                   "cudaMemcpy (recovery slices)");
+                detail::copy_to_host(rec.get(), out.slice(0), r * bs);
             }
         }
         stats_.ms_gpu = ms_since(t2);
@@ -397,7 +560,7 @@ class Par2Creator {
             h.update(set_id.data(), 16);
             h.update(packet_types::RECV_SLICE.data(), 16);
             h.update(ex, 4);
-            h.update(rec.data() + e * bs, bs);
+            h.update(rec.get() + e * bs, bs);
             const FileHash md5 = h.finalize();
             const uint64_t len = 64 + 4 + bs;
             memcpy(hd, kPar2Magic, 8);
@@ -408,18 +571,24 @@ class Par2Creator {
             memcpy(hd + 48, packet_types::RECV_SLICE.data(), 16);
             memcpy(hd + 64, ex, 4);
         });
-        std::vector<std::filesystem::path> written;
-        for (const VolumeInfo &v : vols) {
+        // the volumes are independent files: written side by side
+        std::vector<uint8_t> vol_ok(vols.size(), 0);
+        detail::parallel_for(vols.size(), [&](size_t i) {
+            const VolumeInfo &v = vols[i];
             FILE *f = fopen(v.path.string().c_str(), "wb");
             bool ok = f && fwrite(common.data(), 1, common.size(), f) == common.size();
             for (uint32_t e : v.exponents)
                 ok = ok && fwrite(head[e].data(), 1, 68, f) == 68 &&
-                     fwrite(rec.data() + static_cast<size_t>(e) * bs, 1, bs, f) == bs;
+                     fwrite(rec.get() + static_cast<size_t>(e) * bs, 1, bs, f) == bs;
             if (f)
                 ok = fclose(f) == 0 && ok;
-            if (!ok)
-                throw Par2Error("Failed to write " + v.path.string());
-            written.push_back(v.path);
+            vol_ok[i] = ok;
+        });
+        std::vector<std::filesystem::path> written;
+        for (size_t i = 0; i < vols.size(); ++i) {
+            if (!vol_ok[i])
+                throw Par2Error("Failed to write " + vols[i].path.string());
+            written.push_back(vols[i].path);
         }
         stats_.files_written = written.size();
         stats_.ms_write = ms_since(t3);
@@ -641,16 +810,11 @@ class Par2Repairer {
                 if (!touched)
                     continue;
                 check_cancel();
-                std::vector<uint8_t> bytes(f.length);
-                if (f.length)
-                    detail::cuda_check(cudaMemcpy(bytes.data(), dev.slice(first[i]), f.length,
-                                                  cudaMemcpyDeviceToHost),
-                                       "cudaMemcpy (repaired file)");
                 const std::filesystem::path fin = dir_ / f.name;
                 std::filesystem::path tmp = fin;
                 tmp += ".par2tmp";
                 commits.emplace_back(tmp, fin);
-                detail::write_file(tmp, bytes.data(), bytes.size());
+                detail::write_file_from_device(tmp, dev.slice(first[i]), f.length);
             }
             check_cancel();
         } catch (...) {
