@@ -463,15 +463,20 @@ class Par2File {
     std::vector<uint8_t> read_recovery(const RecoveryRef &r, uint64_t offset, uint64_t n) const
     {
         std::vector<uint8_t> out(n);
+        read_recovery_into(r, offset, n, out.data());
+        return out;
+    }
+    // The same into caller memory (safe to call from several threads).
+    void read_recovery_into(const RecoveryRef &r, uint64_t offset, uint64_t n, uint8_t *out) const
+    {
         FILE *f = fopen(r.file.string().c_str(), "rb");
         if (!f || fseeko(f, static_cast<off_t>(r.data_offset + offset), SEEK_SET) != 0 ||
-            fread(out.data(), 1, n, f) != n) {
+            (n && fread(out, 1, n, f) != n)) {
             if (f)
                 fclose(f);
             throw Par2Error("Failed to read recovery slice from " + r.file.string());
         }
         fclose(f);
-        return out;
     }
 
   private:

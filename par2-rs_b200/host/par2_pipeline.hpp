@@ -333,6 +333,47 @@ template <class Sink> bool drain_device(const uint8_t *d, size_t n, Sink sink)
     return !failed;
 }
 
+// Uploads n pieces: fill(i, pinned host chunk) writes piece i (at most
+// kPinnedChunk bytes) into the chunk and returns {device destination, bytes}.
+// Up to 8 host threads each run fills and copies through their own pooled
+// chunk and stream, so the reads of several pieces and their uploads overlap.
+template <class Fill> void fill_device(size_t n, Fill fill)
+{
+    const size_t nt = std::min<size_t>(n, std::min(8u, std::max(1u, std::thread::hardware_concurrency())));
+    std::atomic<size_t> next{0};
+    std::vector<std::string> errors(nt);
+    auto worker = [&](size_t t) {
+        uint8_t *buf = nullptr;
+        cudaStream_t st = nullptr;
+        try {
+            buf = PinnedPool::get().take();
+            cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+            for (size_t i; errors[t].empty() && (i = next.fetch_add(1)) < n;) {
+                const std::pair<uint8_t *, size_t> dst = fill(i, buf);
+                cuda_check(cudaMemcpyAsync(dst.first, buf, dst.second, cudaMemcpyHostToDevice, st),
+                           "cudaMemcpyAsync");
+                cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+            }
+        } catch (const std::exception &e) {
+            errors[t] = e.what();
+            next = n;  // the other threads stop too
+        }
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+        PinnedPool::get().give(buf);
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; ++t)
+        pool.emplace_back(worker, t);
+    for (auto &th : pool)
+        th.join();
+    for (const std::string &e : errors)
+        if (!e.empty())
+            throw Par2Error(e);
+}
+
 // Copies n bytes of device memory into host memory h (any, pageable).
 inline void copy_to_host(uint8_t *h, const uint8_t *d, size_t n)
 {
@@ -753,12 +794,16 @@ class Par2Repairer {
         // the m lowest exponents' slices to the device, then the repair there
         detail::DeviceSlices rdev(m, bs), out(m, bs);
         std::vector<uint32_t> exps(m);
-        for (uint64_t q = 0; q < m; ++q) {
-            const std::vector<uint8_t> d = p.read_recovery(recs[q], 0, bs);
-            detail::cuda_check(cudaMemcpy(rdev.slice(q), d.data(), bs, cudaMemcpyHostToDevice),
-                               "cudaMemcpy (recovery slice)");
+        for (uint64_t q = 0; q < m; ++q)
             exps[q] = recs[q].exponent;
-        }
+        // pieces of up to one pinned chunk, read and uploaded by several threads
+        const uint64_t parts = (bs + detail::kPinnedChunk - 1) / detail::kPinnedChunk;
+        detail::fill_device(m * parts, [&](size_t i, uint8_t *host) {
+            const uint64_t q = i / parts, off = (i % parts) * detail::kPinnedChunk;
+            const size_t len = static_cast<size_t>(std::min<uint64_t>(detail::kPinnedChunk, bs - off));
+            p.read_recovery_into(recs[q], off, len, host);
+            return std::make_pair(rdev.slice(q) + off, len);
+        });
         check_cancel();
         std::set<uint64_t> dset(damaged.begin(), damaged.end());
         std::vector<const uint8_t *> present;
