@@ -746,17 +746,31 @@ def run_batched(args):
             x["out_plain"] = torch.zeros((m, x["S"]), dtype=torch.uint8, device=dev)
             x["out_batch"] = torch.zeros_like(x["out_plain"])
 
+    # each set's slice tables (device addresses, uint64), built once as a
+    # caller holds them: neither arm times Python list building
+    def rows(t, keep=None):
+        a = np.uint64(t.data_ptr()) + np.arange(t.shape[0], dtype=np.uint64) * \
+            np.uint64(t.stride(0))
+        return a if keep is None else a[keep]
+
+    for x in sets:
+        x["t_src"] = rows(x["src"])
+        x["t_out_plain"] = rows(x["out_plain"])
+        x["t_out_batch"] = rows(x["out_batch"])
+        if not x["create"]:
+            keep = np.ones(x["k"], bool)
+            keep[x["missing"]] = False
+            x["t_present"] = rows(x["src"], keep)
+            x["t_rec"] = rows(x["rec"])
+
     def plain_all():
         for x in sets:
             k, S = x["k"], x["S"]
             if x["create"]:
-                ctx.encode([x["src"][i] for i in range(k)], S, np.arange(x["r"]),
-                           [x["out_plain"][e] for e in range(x["r"])], device=True)
+                ctx.encode(x["t_src"], S, np.arange(x["r"]), x["t_out_plain"], device=True)
             else:
-                mset = set(x["missing"].tolist())
-                ctx.repair(k, S, x["missing"], [x["src"][i] for i in range(k) if i not in mset],
-                           np.arange(x["m"]), [x["rec"][q] for q in range(x["m"])],
-                           [x["out_plain"][q] for q in range(x["m"])], device=True)
+                ctx.repair(k, S, x["missing"], x["t_present"], np.arange(x["m"]), x["t_rec"],
+                           x["t_out_plain"], device=True)
 
     def jobs_for(xs):
         jobs = []
@@ -764,17 +778,13 @@ def run_batched(args):
             k, S = x["k"], x["S"]
             if x["create"]:
                 jobs.append({"kind": par2gpu.JOB_CREATE, "k": k, "slice_bytes": S,
-                             "src": [x["src"].data_ptr() + i * S for i in range(k)],
-                             "exps": np.arange(x["r"]),
-                             "out": [x["out_batch"].data_ptr() + e * S for e in range(x["r"])]})
+                             "src": x["t_src"], "exps": np.arange(x["r"]),
+                             "out": x["t_out_batch"]})
             else:
-                mset = set(x["missing"].tolist())
                 jobs.append({"kind": par2gpu.JOB_REPAIR, "k": k, "slice_bytes": S,
-                             "src": [x["src"].data_ptr() + i * S for i in range(k)
-                                     if i not in mset],
-                             "missing": x["missing"], "exps": np.arange(x["m"]),
-                             "recovery": [x["rec"].data_ptr() + q * S for q in range(x["m"])],
-                             "out": [x["out_batch"].data_ptr() + q * S for q in range(x["m"])]})
+                             "src": x["t_present"], "missing": x["missing"],
+                             "exps": np.arange(x["m"]), "recovery": x["t_rec"],
+                             "out": x["t_out_batch"]})
         return jobs
 
     # groups whose scratch (bit planes + records) fits the budget
@@ -833,6 +843,14 @@ def run_batched(args):
     ms = e0.elapsed_time(e1)
     out["graph_replay"] = {"makespan_ms": ms, "jobs_per_s": len(sets) / (ms * 1e-3),
                            "note": "decode matrices precomputed; device work only"}
+    # the multiply-accumulate work of all sets (create: k x r, repair: one
+    # pass of k sources x m outputs) against the LOP3 roofline, per arm
+    macs = sum(x["k"] * (x["r"] if x["create"] else x["m"]) * (x["S"] // 2) for x in sets)
+    int_peak, _ = probe_int_peak(0)
+    out["symbol_macs"] = macs
+    for name in ("plain", "batched", "graph_replay"):
+        if int_peak:
+            out[name]["int_frac"] = 2.0 * macs / (out[name]["makespan_ms"] * 1e-3) / int_peak
     for b in graphs:
         b.close()
     same = all(torch.equal(x["out_plain"], x["out_batch"]) for x in sets)

@@ -243,18 +243,17 @@ def serve_one_at_a_time(ctx, jobs, arrivals):
         if wait > 0:
             time.sleep(wait)
         _alloc_outputs(job)
-        S, base = job.S, job.src.data_ptr()
+        S = job.S
+        # slice tables as address arrays (what a caller holds; no per-slice
+        # Python objects)
         if job.kind == "create":
-            ctx.encode([base + i * S for i in range(job.k)], S, np.arange(job.r),
-                       [job.out.data_ptr() + e * S for e in range(job.r)], device=True)
+            ctx.encode(_rows(job.src), S, np.arange(job.r), _rows(job.out), device=True)
         elif job.kind == "verify":
-            job.md5, job.crc = ctx.hash_slices([base + i * S for i in range(job.k)], S,
-                                               device=True)
+            job.md5, job.crc = ctx.hash_slices(_rows(job.src), S, device=True)
         else:
-            miss = set(job.missing.tolist())
-            ctx.repair(job.k, S, job.missing, [base + i * S for i in range(job.k) if i not in miss],
-                       np.arange(job.m), [job.rec.data_ptr() + q * S for q in range(job.m)],
-                       [job.out.data_ptr() + q * S for q in range(job.m)], device=True)
+            present = np.setdiff1d(np.arange(job.k), job.missing)
+            ctx.repair(job.k, S, job.missing, _rows(job.src, present), np.arange(job.m),
+                       _rows(job.rec), _rows(job.out), device=True)
         lat[idx] = (time.perf_counter() - t0) - arrivals[idx]
     return lat, time.perf_counter() - t0
 
