@@ -606,51 +606,69 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
         P2G_TRY(muladd_run(ctx, d_src, static_cast<int>(k), d_dst, static_cast<int>(r),
                            slice_bytes, ctx->recs.as<uint32_t>(), 0));
     } else {
-        const int full = tail ? groups - kTailGroups : groups;
-        for (int g = 0; g < full; ++g) {
-            const size_t i0 = k * g / groups, i1 = k * (g + 1) / groups;
-            P2G_TRY(copy_slices(s.data() + i0, src + i0, i1 - i0, slice_bytes,
-                                cudaMemcpyHostToDevice, ctx->copy_stream));
-            P2G_CUDA(cudaEventRecord(ctx->pipe_ev[g], ctx->copy_stream));
-            P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
-            P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
-                               static_cast<int>(r), slice_bytes,
-                               ctx->recs.as<uint32_t>() + i0 * r * 16, g == 0 ? 0 : 1));
-        }
-        if (tail) {
-            uint8_t *const *tab = reinterpret_cast<uint8_t *const *>(dp + tail_off);
-            std::vector<const uint8_t *> hs(ntail);
-            std::vector<uint8_t *> ds(ntail), uo(r), so(r);
-            cudaEvent_t *up = ctx->pipe_ev + kSlabEvents, *done = up + slabs;
-            for (int q = 0; q < slabs; ++q) {
-                const size_t w = cut[q + 1] - cut[q];
-                for (size_t i = 0; i < ntail; ++i) {
-                    hs[i] = src[t0 + i] + cut[q];
-                    ds[i] = s[t0 + i] + cut[q];
-                }
-                P2G_TRY(copy_slices(ds.data(), hs.data(), ntail, w, cudaMemcpyHostToDevice,
-                                    ctx->copy_stream));
-                P2G_CUDA(cudaEventRecord(up[q], ctx->copy_stream));
-                P2G_CUDA(cudaStreamWaitEvent(ctx->stream, up[q], 0));
-                const uint8_t *const *qs = reinterpret_cast<const uint8_t *const *>(tab + q * (ntail + r));
-                P2G_TRY(muladd_run(ctx, qs, static_cast<int>(ntail), tab + q * (ntail + r) + ntail,
-                                   static_cast<int>(r), w, ctx->recs.as<uint32_t>() + t0 * r * 16, 1));
-                P2G_CUDA(cudaEventRecord(done[q], ctx->stream));
-                P2G_CUDA(cudaStreamWaitEvent(ctx->d2h_stream, done[q], 0));
-                for (size_t e = 0; e < r; ++e) {
-                    uo[e] = out[e] + cut[q];
-                    so[e] = d[e] + cut[q];
-                }
-                P2G_TRY(copy_slices(uo.data(), so.data(), r, w, cudaMemcpyDeviceToHost,
-                                    ctx->d2h_stream));
+        // The copies run on the context's side streams.  If a step below
+        // fails, the ones already enqueued (some into the caller's host
+        // buffers) finish before the error is returned.
+        const int rc = [&]() -> int {
+            const int full = tail ? groups - kTailGroups : groups;
+            for (int g = 0; g < full; ++g) {
+                const size_t i0 = k * g / groups, i1 = k * (g + 1) / groups;
+                P2G_TRY(copy_slices(s.data() + i0, src + i0, i1 - i0, slice_bytes,
+                                    cudaMemcpyHostToDevice, ctx->copy_stream));
+                P2G_CUDA(cudaEventRecord(ctx->pipe_ev[g], ctx->copy_stream));
+                P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
+                P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
+                                   static_cast<int>(r), slice_bytes,
+                                   ctx->recs.as<uint32_t>() + i0 * r * 16, g == 0 ? 0 : 1));
             }
-            // the call ends when the last read-back has landed
-            P2G_CUDA(cudaEventRecord(done[slabs], ctx->d2h_stream));
-            P2G_CUDA(cudaStreamWaitEvent(ctx->stream, done[slabs], 0));
+            if (tail) {
+                uint8_t *const *tab = reinterpret_cast<uint8_t *const *>(dp + tail_off);
+                std::vector<const uint8_t *> hs(ntail);
+                std::vector<uint8_t *> ds(ntail), uo(r), so(r);
+                cudaEvent_t *up = ctx->pipe_ev + kSlabEvents, *done = up + slabs;
+                for (int q = 0; q < slabs; ++q) {
+                    const size_t w = cut[q + 1] - cut[q];
+                    for (size_t i = 0; i < ntail; ++i) {
+                        hs[i] = src[t0 + i] + cut[q];
+                        ds[i] = s[t0 + i] + cut[q];
+                    }
+                    P2G_TRY(copy_slices(ds.data(), hs.data(), ntail, w, cudaMemcpyHostToDevice,
+                                        ctx->copy_stream));
+                    P2G_CUDA(cudaEventRecord(up[q], ctx->copy_stream));
+                    P2G_CUDA(cudaStreamWaitEvent(ctx->stream, up[q], 0));
+                    uint8_t *const *qt = tab + q * (ntail + r);
+                    P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(qt),
+                                       static_cast<int>(ntail), qt + ntail, static_cast<int>(r), w,
+                                       ctx->recs.as<uint32_t>() + t0 * r * 16, 1));
+                    P2G_CUDA(cudaEventRecord(done[q], ctx->stream));
+                    P2G_CUDA(cudaStreamWaitEvent(ctx->d2h_stream, done[q], 0));
+                    for (size_t e = 0; e < r; ++e) {
+                        uo[e] = out[e] + cut[q];
+                        so[e] = d[e] + cut[q];
+                    }
+                    P2G_TRY(copy_slices(uo.data(), so.data(), r, w, cudaMemcpyDeviceToHost,
+                                        ctx->d2h_stream));
+                }
+                // the call ends when the last read-back has landed
+                P2G_CUDA(cudaEventRecord(done[slabs], ctx->d2h_stream));
+                P2G_CUDA(cudaStreamWaitEvent(ctx->stream, done[slabs], 0));
+            }
+            return P2G_OK;
+        }();
+        if (rc != P2G_OK) {
+            cudaStreamSynchronize(ctx->copy_stream);
+            cudaStreamSynchronize(ctx->d2h_stream);
+            cudaStreamSynchronize(ctx->stream);
+            return rc;
         }
     }
-    if (d_staged && !tail)
-        P2G_TRY(unstage(ctx, out, d, r, slice_bytes, dev));
+    if (d_staged && !tail) {
+        const int rc = unstage(ctx, out, d, r, slice_bytes, dev);
+        if (rc != P2G_OK) {
+            cudaStreamSynchronize(ctx->stream);  // copies already enqueued land first
+            return rc;
+        }
+    }
     return finish(ctx);
 }
 
