@@ -183,11 +183,18 @@ static int stage(p2g_ctx *ctx, p2g::DevBuf &buf, const uint8_t *const *ptrs, siz
     return P2G_OK;
 }
 
+// Copies results back to the caller's slices.  If a copy fails, the ones
+// already enqueued land before the error is returned (the caller may free
+// its buffers as soon as the call returns).
 static int unstage(p2g_ctx *ctx, uint8_t *const *user, const std::vector<uint8_t *> &dev,
                    size_t n, size_t bytes, bool device)
 {
-    return copy_slices(user, dev.data(), n, bytes,
-                       device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream);
+    const int rc = copy_slices(user, dev.data(), n, bytes,
+                               device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               ctx->stream);
+    if (rc != P2G_OK)
+        cudaStreamSynchronize(ctx->stream);
+    return rc;
 }
 
 // Starts a call: resets the launch counter and the timing marks.
@@ -662,13 +669,8 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
             return rc;
         }
     }
-    if (d_staged && !tail) {
-        const int rc = unstage(ctx, out, d, r, slice_bytes, dev);
-        if (rc != P2G_OK) {
-            cudaStreamSynchronize(ctx->stream);  // copies already enqueued land first
-            return rc;
-        }
-    }
+    if (d_staged && !tail)
+        P2G_TRY(unstage(ctx, out, d, r, slice_bytes, dev));
     return finish(ctx);
 }
 
