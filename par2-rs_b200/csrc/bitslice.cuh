@@ -111,4 +111,75 @@ __host__ __device__ __forceinline__ void make_record(uint32_t c, uint32_t w[16])
             w[4 * m + i] = row_offset(m, n0, n1, 2 * i) | (row_offset(m, n0, n1, 2 * i + 1) << 16);
 }
 
+// Words per record of the two table forms.
+constexpr int kRecordWords = 16;
+constexpr int kRecordWordsSmall = 24;
+
+// The small-output form (6 + 5 + 5 planes): three tables of 64, 32 and 32
+// rows over planes 0-5, 6-10 and 11-15 (T1 from row 64, T2 from row 96), 16
+// KiB per input instead of 64, built with 128 row stores instead of 512 --
+// cheaper when few outputs share an input's tables, at 48 row reads per
+// coefficient instead of 32.  Output plane j is
+//   T0[a_j] ^ T1[b_j] ^ T2[c_j],  a_j = sum_{b<6} bit_j(c x^b) << b,
+//   b_j = sum_{b<5} bit_j(c x^{6+b}) << b,  c_j = sum_{b<5} bit_j(c x^{11+b}) << b.
+// The 48 rows form the sequence s = 3j + t (t = 0, 1, 2 for T0, T1, T2),
+// fetched four at a time: ldmatrix k reads s = 4k..4k+3, lane group m
+// (lanes 8m..8m+7) pointing at row 4k + m.  Words 6m..6m+5 of the 24-word
+// record hold lane group m's twelve byte offsets: k = 2i in the low half of
+// word 6m + i, k = 2i + 1 in the high half.
+__host__ __device__ __forceinline__ void make_record_small(uint32_t c, uint32_t w[24])
+{
+    uint32_t col[16];
+    uint32_t v = c & 0xFFFFu;
+#pragma unroll
+    for (int b = 0; b < 16; ++b) {
+        col[b] = v;
+        v = gf_times_x(v);
+    }
+    uint32_t off[48];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        uint32_t a = 0, b1 = 0, c1 = 0;
+#pragma unroll
+        for (int b = 0; b < 6; ++b)
+            a |= ((col[b] >> j) & 1u) << b;
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {
+            b1 |= ((col[6 + b] >> j) & 1u) << b;
+            c1 |= ((col[11 + b] >> j) & 1u) << b;
+        }
+        off[3 * j] = a * kRowBytes;
+        off[3 * j + 1] = (64u + b1) * kRowBytes;
+        off[3 * j + 2] = (96u + c1) * kRowBytes;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+            w[6 * m + i] = off[8 * i + m] | (off[8 * i + 4 + m] << 16);
+}
+
+#ifdef __CUDACC__
+// Writes record idx of coefficient c in the small (24-word) or the 8 + 8
+// (16-word) form; records are 16-byte aligned in both.
+__device__ __forceinline__ void write_record(uint32_t *recs, size_t idx, uint32_t c, bool small)
+{
+    if (small) {
+        uint32_t w[kRecordWordsSmall];
+        make_record_small(c, w);
+        uint4 *R = reinterpret_cast<uint4 *>(recs + idx * kRecordWordsSmall);
+#pragma unroll
+        for (int q = 0; q < kRecordWordsSmall / 4; ++q)
+            R[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+        return;
+    }
+    uint32_t w[kRecordWords];
+    make_record(c, w);
+    uint4 *R = reinterpret_cast<uint4 *>(recs + idx * kRecordWords);
+#pragma unroll
+    for (int q = 0; q < kRecordWords / 4; ++q)
+        R[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+}
+#endif
+
 }  // namespace p2g

@@ -250,7 +250,7 @@ static int matrix_muladd(p2g_ctx *ctx, const std::vector<uint8_t *> &src,
     memcpy(h + L.a_off, coeff, nin * nout * 2);
     P2G_TRY(upload_params(ctx, L));
     uint8_t *d = ctx->params.as<uint8_t>();
-    P2G_TRY(ctx->recs.ensure(nin * nout * 64));
+    P2G_TRY(ctx->recs.ensure(record_bytes(nin, static_cast<int>(nout))));
     P2G_TRY(records_from_matrix(ctx, reinterpret_cast<const uint16_t *>(d + L.a_off),
                                 static_cast<int>(nin), static_cast<int>(nout),
                                 ctx->recs.as<uint32_t>()));
@@ -498,6 +498,7 @@ int p2g_set_plan(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes,
     p.psplit = plan->warps_per_group;
     p.nblk = plan->output_blocks;
     p.nsplit = plan->input_splits;
+    p.small = nout <= static_cast<size_t>(p2g::kSmallOutputs);  // the table form follows nout
     if (nin > 65535 || nout > 65535 ||
         !plan_valid(p, static_cast<int>(nin), static_cast<int>(nout), slice_bytes)) {
         set_error("p2g_set_plan: warps=%d outputs_per_group=%d warps_per_group=%d blocks=%d "
@@ -603,7 +604,8 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     }
     P2G_TRY(upload_params(ctx, L));
     uint8_t *dp = ctx->params.as<uint8_t>();
-    P2G_TRY(ctx->recs.ensure(k * r * 64));
+    P2G_TRY(ctx->recs.ensure(record_bytes(k, static_cast<int>(r))));
+    const size_t rw = static_cast<size_t>(record_words(static_cast<int>(r)));  // per record
     P2G_TRY(records_par2(ctx, reinterpret_cast<const uint16_t *>(dp + L.a_off),
                          reinterpret_cast<const uint32_t *>(dp + L.b_off), static_cast<int>(k),
                          static_cast<int>(r), ctx->recs.as<uint32_t>()));
@@ -626,7 +628,7 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
                 P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
                 P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0), d_dst,
                                    static_cast<int>(r), slice_bytes,
-                                   ctx->recs.as<uint32_t>() + i0 * r * 16, g == 0 ? 0 : 1));
+                                   ctx->recs.as<uint32_t>() + i0 * r * rw, g == 0 ? 0 : 1));
             }
             if (tail) {
                 uint8_t *const *tab = reinterpret_cast<uint8_t *const *>(dp + tail_off);
@@ -646,7 +648,7 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
                     uint8_t *const *qt = tab + q * (ntail + r);
                     P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(qt),
                                        static_cast<int>(ntail), qt + ntail, static_cast<int>(r), w,
-                                       ctx->recs.as<uint32_t>() + t0 * r * 16, 1));
+                                       ctx->recs.as<uint32_t>() + t0 * r * rw, 1));
                     P2G_CUDA(cudaEventRecord(done[q], ctx->stream));
                     P2G_CUDA(cudaStreamWaitEvent(ctx->d2h_stream, done[q], 0));
                     for (size_t e = 0; e < r; ++e) {
@@ -919,7 +921,7 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
     }
     // 2. RHS = R ^ V * present
     if (np) {
-        P2G_TRY(ctx->recs.ensure(np * m * 64));
+        P2G_TRY(ctx->recs.ensure(record_bytes(np, static_cast<int>(m))));
         P2G_TRY(records_par2(ctx, reinterpret_cast<const uint16_t *>(dp + L.b_off), d_exps,
                              static_cast<int>(np), static_cast<int>(m), ctx->recs.as<uint32_t>()));
         P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.src_off),
@@ -928,7 +930,7 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
                            static_cast<int>(m), slice_bytes, ctx->recs.as<uint32_t>(), 1));
     }
     // 3. missing = A^-1 * RHS
-    P2G_TRY(ctx->recs2.ensure(m * m * 64));
+    P2G_TRY(ctx->recs2.ensure(record_bytes(m, static_cast<int>(m))));
     P2G_TRY(records_from_matrix(ctx, ctx->inv.as<uint16_t>(), static_cast<int>(m),
                                 static_cast<int>(m), ctx->recs2.as<uint32_t>()));
     P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.dst_off),

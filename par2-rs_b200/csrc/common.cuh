@@ -42,6 +42,7 @@ struct MuladdPlan {
     int nblk = 1;
     int nsplit = 1;
     int psplit = 1;  // warps sharing one output group (each holds 16/psplit planes)
+    bool small = false;  // small-output tables (set for problems of <= kSmallOutputs outputs)
 };
 
 using PlanKey = std::tuple<int, int, size_t>;  // inputs, outputs, slice bytes

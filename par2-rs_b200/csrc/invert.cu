@@ -484,12 +484,7 @@ __global__ void gj_records_rows(const uint16_t *__restrict__ M, int W, const int
     if (gid >= static_cast<size_t>(nin) * nout)
         return;
     const int o = static_cast<int>(gid % nout), i = static_cast<int>(gid / nout);
-    uint32_t w[16];
-    make_record(M[static_cast<size_t>(orow[o]) * W + c0 + i], w);
-    uint4 *R = reinterpret_cast<uint4 *>(recs + gid * 16);
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-        R[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+    write_record(recs, gid, M[static_cast<size_t>(orow[o]) * W + c0 + i], nout <= kSmallOutputs);
 }
 
 // M[K_j, :] = X_j
@@ -856,7 +851,8 @@ static int woodbury_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_x,
         d_x, m, g, reinterpret_cast<const uint32_t *>(b + o_e),
         reinterpret_cast<const uint32_t *>(b + o_h), Wm, ctx->d_log, ctx->d_exp);
     P2G_CUDA(cudaGetLastError());
-    const size_t nrec = static_cast<size_t>(m) * g * 64;
+    // the three products' records (g, g and m outputs) share one buffer
+    const size_t nrec = std::max({record_bytes(m, g), record_bytes(g, g), record_bytes(g, m)});
     P2G_TRY(ctx->recs2.ensure(nrec));
     uint32_t *recs = ctx->recs2.as<uint32_t>();
     const size_t bytes = static_cast<size_t>(m) * 2;
@@ -950,9 +946,14 @@ int gj_invert(p2g_ctx *ctx, GjWork &w, int m, const uint16_t *d_cmiss, const uin
     }
     P2G_CUDA(cudaFuncSetAttribute(gj_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(kExpSmem)));
-    P2G_TRY(ctx->recs2.ensure(static_cast<size_t>(kPanel) * m * 64 + kPanel * kPanel * 64));
+    // per panel: the b x b pivot block's records, then the b x (m - b) row
+    // update's, each in the form for its output count (b, m - b <= m)
+    const size_t recA_bytes = std::max(record_bytes(kPanel, kPanel),
+                                       record_bytes(kSmallOutputs, kSmallOutputs));
+    P2G_TRY(ctx->recs2.ensure(recA_bytes +
+                              std::max(record_bytes(kPanel, m), record_bytes(kPanel, kSmallOutputs))));
     uint32_t *recsA = ctx->recs2.as<uint32_t>();
-    uint32_t *recsO = recsA + kPanel * kPanel * 16;
+    uint32_t *recsO = recsA + recA_bytes / 4;
     for (int c0 = 0; c0 < m; c0 += kPanel) {
         const int b = std::min(kPanel, m - c0);
         gj_panel<<<1, kGjThreads, kExpSmem, ctx->stream>>>(M, m, W, c0, b, pb, status,

@@ -26,6 +26,11 @@
 //     double-buffered, one CTA barrier per input slice.
 //   * Few tiles / outputs: the input range is split across CTAs and the
 //     partial sums are folded into the output with atomic XOR.
+//   * Problems of at most 24 outputs use three tables instead (planes 0-5,
+//     6-10, 11-15: 64 + 32 + 32 rows, 16 KiB), built with 128 row stores per
+//     input instead of 512 at 48 row reads per coefficient instead of 32;
+//     with few outputs to share an input's tables the build dominates, and
+//     the smaller tables let two CTAs share an SM.
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -41,6 +46,8 @@ namespace p2g {
 constexpr int kTileBytes = 2048;             // 1024 symbols
 constexpr int kTableWords = 512 * 32;        // T0 and T1, 128 B per row
 constexpr int kTableBytes = kTableWords * 4; // 64 KiB
+constexpr int kSmallTableWords = 128 * 32;   // T0, T1, T2 of the small-output form
+constexpr int kSmallTableBytes = kSmallTableWords * 4;  // 16 KiB
 constexpr int kRing = 4;
 
 // Four 8x8 b16 matrices from shared memory: lanes 8m..8m+7 give the row
@@ -150,16 +157,6 @@ __global__ void slices_to_planes(const uint8_t *const *__restrict__ src, int nin
         P[b * 32] = x[b];
 }
 
-__device__ __forceinline__ void put_record(uint32_t *recs, size_t idx, uint32_t c)
-{
-    uint32_t w[16];
-    make_record(c, w);
-    uint4 *R = reinterpret_cast<uint4 *>(recs + idx * 16);
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-        R[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-}
-
 __global__ void records_matrix_kernel(const uint16_t *__restrict__ coeff, int nin, int nout,
                                       uint32_t *__restrict__ recs)
 {
@@ -168,7 +165,7 @@ __global__ void records_matrix_kernel(const uint16_t *__restrict__ coeff, int ni
         return;
     int o = static_cast<int>(gid % nout);
     size_t i = gid / nout;
-    put_record(recs, gid, coeff[static_cast<size_t>(o) * nin + i]);
+    write_record(recs, gid, coeff[static_cast<size_t>(o) * nin + i], nout <= kSmallOutputs);
 }
 
 // c_i^e by the log / antilog tables: (log c * e) mod 65535 (galois/core.rs:242-258)
@@ -192,28 +189,32 @@ __global__ void records_par2_kernel(const uint16_t *__restrict__ consts,
         c = 1u;
     else
         c = gexp[static_cast<uint32_t>((static_cast<uint64_t>(glog[base]) * e) % 65535u)];
-    put_record(recs, gid, c);
+    write_record(recs, gid, c, nout <= kSmallOutputs);
 }
 
 // WARPS warps per CTA; each output group of EREG outputs is held by PSPLIT
 // warps, each keeping 16 / PSPLIT of the 16 planes (PSPLIT = 2 doubles the
-// warps per SM at the same number of outputs per table).
+// warps per SM at the same number of outputs per table).  SMALL selects the
+// small-output tables (6 + 5 + 5 planes, 24-word records; 8 warps, PSPLIT 1).
 // One work item: column tile t, output block ob, inputs [i0, i1).  smode:
 // 0 store, 1 XOR into the outputs, 2 atomic XOR (input ranges of one tile
 // and block handled by several CTAs).
-template <int WARPS, int EREG, int PSPLIT>
+template <int WARPS, int EREG, int PSPLIT, bool SMALL = false>
 __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__restrict__ planes,
                                             const uint32_t *__restrict__ recs, int nin, int nout,
                                             int T, int t, int ob, int i0, int i1,
                                             uint8_t *const *__restrict__ dst, size_t S, int smode)
 {
+    static_assert(!SMALL || (WARPS == 8 && PSPLIT == 1), "small tables: 8 warps, no plane split");
     constexpr int THREADS = WARPS * 32;
     constexpr int GROUPS = WARPS / PSPLIT;   // output groups
     constexpr int NPL = 16 / PSPLIT;         // planes per warp
     constexpr int EBLK = GROUPS * EREG;
-    constexpr int SLOT = kTileBytes + EBLK * 64;
+    constexpr int RW = SMALL ? kRecordWordsSmall : kRecordWords;  // words per record
+    constexpr int TW = SMALL ? kSmallTableWords : kTableWords;   // words per table buffer
+    constexpr int SLOT = kTileBytes + EBLK * RW * 4;
     uint32_t *tab = reinterpret_cast<uint32_t *>(smem);
-    uint8_t *ring = smem + 2 * kTableBytes;
+    uint8_t *ring = smem + 2 * TW * 4;
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -231,8 +232,8 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
             const uint8_t *gp = reinterpret_cast<const uint8_t *>(
                 planes + (static_cast<size_t>(i) * T + t) * 512);
             const uint8_t *gr = reinterpret_cast<const uint8_t *>(
-                recs + (static_cast<size_t>(i) * nout + obase) * 16);
-            const int nchunk = 128 + nb * 4;
+                recs + (static_cast<size_t>(i) * nout + obase) * RW);
+            const int nchunk = 128 + nb * (RW / 4);
             for (int c = threadIdx.x; c < nchunk; c += THREADS) {
                 if (c < 128)
                     cp_async16(s + c * 16, gp + c * 16);
@@ -248,7 +249,54 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
     // row's low nibble the pattern of its planes 0-3).  Warp w builds groups
     // [32w/WARPS, 32(w+1)/WARPS), which never straddle the two halves for
     // WARPS in {8, 12, 16}.
+    // Small form: warp w builds 16 rows -- warps 0-3 the four quarters of T0
+    // (planes 0-3 vary, planes 4-5 fixed by w), warps 4-5 the halves of T1
+    // (planes 6-9 vary, plane 10 fixed), warps 6-7 those of T2 (planes 11-14,
+    // plane 15).
+    auto build_small = [&](int i, int buf) {
+        const uint32_t *P = reinterpret_cast<const uint32_t *>(ring + (i & (kRing - 1)) * SLOT);
+        int b0, row0;
+        uint32_t H;
+        if (warp < 4) {
+            b0 = 0;
+            row0 = 16 * warp;
+            H = ((warp & 1) ? P[4 * 32 + lane] : 0u) ^ ((warp & 2) ? P[5 * 32 + lane] : 0u);
+        } else if (warp < 6) {
+            b0 = 6;
+            row0 = 64 + 16 * (warp - 4);
+            H = (warp & 1) ? P[10 * 32 + lane] : 0u;
+        } else {
+            b0 = 11;
+            row0 = 96 + 16 * (warp - 6);
+            H = (warp & 1) ? P[15 * 32 + lane] : 0u;
+        }
+        uint32_t p[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            p[b] = P[(b0 + b) * 32 + lane];
+        uint32_t L[16];
+        L[0] = 0;
+        L[1] = p[0];
+        L[2] = p[1];
+        L[3] = p[0] ^ p[1];
+        L[4] = p[2];
+        L[5] = L[4] ^ p[0];
+        L[6] = L[4] ^ p[1];
+        L[7] = L[6] ^ p[0];
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+            L[8 + x] = L[x] ^ p[3];
+        uint32_t *T0 = tab + buf * TW + row0 * 32 + lane;
+#pragma unroll
+        for (int x = 0; x < 16; ++x)
+            T0[x * 32] = H ^ L[x];
+    };
+
     auto build = [&](int i, int buf) {
+        if constexpr (SMALL) {
+            build_small(i, buf);
+            return;
+        }
         const uint32_t *P = reinterpret_cast<const uint32_t *>(ring + (i & (kRing - 1)) * SLOT);
         const int g0 = warp * 32 / WARPS, g1 = (warp + 1) * 32 / WARPS;
         const int half = g0 >> 4;
@@ -270,7 +318,7 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
             L[8 + x] = L[x] ^ p[3];
         constexpr int GMAX = (32 + WARPS - 1) / WARPS;
         const int h0 = g0 & 15;
-        uint32_t *T0 = tab + buf * kTableWords + (half * 256 + h0 * 16) * 32 + lane;
+        uint32_t *T0 = tab + buf * TW + (half * 256 + h0 * 16) * 32 + lane;
 #pragma unroll
         for (int gg = 0; gg < GMAX; ++gg) {
             if (GMAX * WARPS == 32 || g0 + gg < g1) {
@@ -295,7 +343,41 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
     // ldmatrix.x4; it supplies the address of 16-byte chunk (L % 8) of the
     // row of matrix L / 8 (record layout: bitslice.cuh make_record).
     const uint32_t tab_s = static_cast<uint32_t>(__cvta_generic_to_shared(tab)) + (lane & 7) * 16;
+    auto consume_small = [&](int i, int buf) {
+        // lane group m's six record words: 3 x 8 bytes at word 6m of each record
+        const uint2 *R = reinterpret_cast<const uint2 *>(ring + (i & (kRing - 1)) * SLOT +
+                                                         kTileBytes) +
+                         my0 * (RW / 2) + (lane >> 3) * 3;
+        const uint32_t tb = tab_s + buf * TW * 4;
+#pragma unroll
+        for (int e = 0; e < EREG; ++e) {
+            if (e < myn) {
+                uint32_t w[6];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const uint2 r = R[e * (RW / 2) + q];
+                    w[2 * q] = r.x;
+                    w[2 * q + 1] = r.y;
+                }
+                // ldmatrix k: rows 4k..4k+3 of the sequence s = 3j + t
+#pragma unroll
+                for (int k = 0; k < 12; ++k) {
+                    const uint32_t off = (k & 1) ? (w[k >> 1] >> 16) : (w[k >> 1] & 0xFFFFu);
+                    uint32_t d[4];
+                    ldsm_x4(tb + off, d[0], d[1], d[2], d[3]);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        acc[e][(4 * k + q) / 3] ^= d[q];
+                }
+            }
+        }
+    };
+
     auto consume = [&](int i, int buf) {
+        if constexpr (SMALL) {
+            consume_small(i, buf);
+            return;
+        }
         const uint4 *R = reinterpret_cast<const uint4 *>(ring + (i & (kRing - 1)) * SLOT +
                                                          kTileBytes) +
                          my0 * 4 + (lane >> 3);
@@ -387,8 +469,8 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
     }
 }
 
-template <int WARPS, int EREG, int PSPLIT>
-__global__ void __launch_bounds__(WARPS * 32, 1)
+template <int WARPS, int EREG, int PSPLIT, bool SMALL = false>
+__global__ void __launch_bounds__(WARPS * 32, SMALL ? 2 : 1)
     muladd_bitsliced(const uint32_t *__restrict__ planes, const uint32_t *__restrict__ recs,
                      int nin, int nout, int T, int nblk, int nsplit,
                      uint8_t *const *__restrict__ dst, size_t S, int mode)
@@ -401,8 +483,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     const int t = bid / nblk;
     const int i0 = static_cast<int>(static_cast<long long>(nin) * split / nsplit);
     const int i1 = static_cast<int>(static_cast<long long>(nin) * (split + 1) / nsplit);
-    muladd_item<WARPS, EREG, PSPLIT>(smem, planes, recs, nin, nout, T, t, ob, i0, i1, dst, S,
-                                     nsplit > 1 ? 2 : mode);
+    muladd_item<WARPS, EREG, PSPLIT, SMALL>(smem, planes, recs, nin, nout, T, t, ob, i0, i1,
+                                            dst, S, nsplit > 1 ? 2 : mode);
 }
 
 // Persistent form for batches of independent problems: one CTA per SM takes
@@ -462,14 +544,17 @@ using KernelFn = void (*)(const uint32_t *, const uint32_t *, int, int, int, int
 
 struct Variant {
     int warps, ereg, psplit;
+    bool small;  // small-output tables (problems of at most kSmallOutputs outputs)
     KernelFn fn;
 };
 
 // Compiled tile shapes: warps per CTA x outputs per warp.  The register
 // budget (64K per SM, one CTA per SM) caps EREG at 13 / 8 / 5 for 8 / 12 / 16
 // warps without spills.
-#define P2G_V(W, E, P) {W, E, P, muladd_bitsliced<W, E, P>}
+#define P2G_V(W, E, P) {W, E, P, false, muladd_bitsliced<W, E, P>}
+#define P2G_VS(E) {8, E, 1, true, muladd_bitsliced<8, E, 1, true>}
 static const Variant kVariants[] = {
+    P2G_VS(1),        P2G_VS(2),        P2G_VS(3),
     P2G_V(8, 1, 1),   P2G_V(8, 2, 1),   P2G_V(8, 3, 1),   P2G_V(8, 4, 1),   P2G_V(8, 5, 1),
     P2G_V(8, 6, 1),   P2G_V(8, 7, 1),   P2G_V(8, 8, 1),   P2G_V(8, 9, 1),   P2G_V(8, 10, 1),
     P2G_V(8, 11, 1),  P2G_V(8, 12, 1),  P2G_V(8, 13, 1),  P2G_V(12, 4, 1),  P2G_V(12, 6, 1),
@@ -477,19 +562,28 @@ static const Variant kVariants[] = {
     P2G_V(16, 5, 1),  P2G_V(16, 8, 2),  P2G_V(16, 10, 2), P2G_V(16, 12, 2),
 };
 #undef P2G_V
+#undef P2G_VS
 
-static KernelFn kernel_for(int warps, int ereg, int psplit)
+static KernelFn kernel_for(int warps, int ereg, int psplit, bool small)
 {
     for (const Variant &v : kVariants)
-        if (v.warps == warps && v.ereg == ereg && v.psplit == psplit)
+        if (v.warps == warps && v.ereg == ereg && v.psplit == psplit && v.small == small)
             return v.fn;
     return nullptr;
 }
+static KernelFn kernel_for(const MuladdPlan &p)
+{
+    return kernel_for(p.warps, p.ereg, p.psplit, p.small);
+}
 
+// The 8 + 8 shapes (the small-output form reuses 8-warp shapes of 1-3
+// outputs per warp).
 int muladd_variants(int *warps, int *eregs, int *psplits, int cap)
 {
     int n = 0;
     for (const Variant &v : kVariants) {
+        if (v.small)
+            continue;
         if (n < cap) {
             warps[n] = v.warps;
             eregs[n] = v.ereg;
@@ -505,7 +599,9 @@ static int block_outputs(const MuladdPlan &p) { return p.warps / p.psplit * p.er
 
 static size_t smem_bytes(const MuladdPlan &p)
 {
-    return 2 * kTableBytes + kRing * (kTileBytes + block_outputs(p) * 64);
+    if (p.small)
+        return 2 * kSmallTableBytes + kRing * (kTileBytes + block_outputs(p) * kRecordWordsSmall * 4);
+    return 2 * kTableBytes + kRing * (kTileBytes + block_outputs(p) * kRecordWords * 4);
 }
 
 // CTAs of plan p that fit on one SM at once (registers and shared memory),
@@ -513,14 +609,14 @@ static size_t smem_bytes(const MuladdPlan &p)
 static int resident_ctas(const MuladdPlan &p)
 {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int>, int> cache;
-    const auto key = std::make_tuple(p.warps, p.ereg, p.psplit);
+    static std::map<std::tuple<int, int, int, bool>, int> cache;
+    const auto key = std::make_tuple(p.warps, p.ereg, p.psplit, p.small);
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end())
         return it->second;
     int n = 0;
-    KernelFn fn = kernel_for(p.warps, p.ereg, p.psplit);
+    KernelFn fn = kernel_for(p);
     const size_t smem = smem_bytes(p);
     if (!fn ||
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -550,8 +646,9 @@ MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t S)
     MuladdPlan p;
     const int T = static_cast<int>((S + kTileBytes - 1) / kTileBytes);
     p.warps = 8;
+    p.small = nout <= kSmallOutputs;
     p.nblk = (nout + 8 * 13 - 1) / (8 * 13);
-    p.ereg = (nout + 8 * p.nblk - 1) / (8 * p.nblk);
+    p.ereg = std::max(1, (nout + 8 * p.nblk - 1) / (8 * p.nblk));
     // Input splits (atomic-XOR folds, whole aligned words: S % 4 == 0) for
     // grids that would leave SMs idle.  A CTA costs its inputs plus a fixed
     // prologue/epilogue of ~17 input tiles (~20 when it folds atomically),
@@ -581,7 +678,8 @@ MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t S)
 
 bool plan_valid(const MuladdPlan &p, int nin, int nout, size_t S)
 {
-    if (p.psplit < 1 || kernel_for(p.warps, p.ereg, p.psplit) == nullptr || p.nblk < 1)
+    if (p.psplit < 1 || p.small != (nout <= kSmallOutputs) || kernel_for(p) == nullptr ||
+        p.nblk < 1)
         return false;
     const long long eb = block_outputs(p);
     return p.nblk * eb >= nout && (p.nblk - 1) * eb < nout && p.nsplit >= 1 &&
@@ -618,7 +716,7 @@ static int launch_kernel(cudaStream_t stream, const MuladdPlan &p, const uint32_
                          const uint32_t *d_recs, int nin, int nout, int T,
                          uint8_t *const *d_dst, size_t S, int mode)
 {
-    KernelFn fn = kernel_for(p.warps, p.ereg, p.psplit);
+    KernelFn fn = kernel_for(p);
     size_t smem = smem_bytes(p);
     P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
@@ -705,7 +803,7 @@ int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdP
     P2G_TRY(ctx->in_copy.ensure(slot * nin));
     P2G_TRY(ctx->out_copy.ensure(slot * nout));
     P2G_TRY(ctx->coeffs.ensure(static_cast<size_t>(nin) * nout * 2 + 16));
-    P2G_TRY(ctx->recs.ensure(static_cast<size_t>(nin) * nout * 64));
+    P2G_TRY(ctx->recs.ensure(record_bytes(nin, nout)));
     P2G_TRY(ctx->planes.ensure(static_cast<size_t>(nin) * T * kTileBytes));
     fill_pattern<<<1024, 256, 0, ctx->stream>>>(ctx->in_copy.as<uint32_t>(), slot * nin / 4, 1u);
     fill_pattern<<<256, 256, 0, ctx->stream>>>(ctx->coeffs.as<uint32_t>(),
@@ -736,15 +834,29 @@ int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdP
     // it allows and the next two, times input splits that keep the grid
     // within a few waves
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    const bool small = nout <= kSmallOutputs;  // the table form is fixed by nout
     std::vector<MuladdPlan> cands;
+    auto add = [&](const MuladdPlan &p) {
+        if (!plan_valid(p, nin, nout, S))
+            return;
+        for (const MuladdPlan &q : cands)
+            if (q.warps == p.warps && q.ereg == p.ereg && q.nblk == p.nblk &&
+                q.nsplit == p.nsplit && q.psplit == p.psplit)
+                return;
+        cands.push_back(p);
+    };
+    // the heuristic's own plan is always a candidate
+    add(choose_plan(nullptr, nin, nout, S));
     for (const Variant &v0 : kVariants) {
+        if (v0.small != small)
+            continue;
         // one pass per (warps, psplit) family: its largest compiled ereg
         // sets the fewest output blocks; then the next two block counts, each
         // with the smallest compiled ereg that covers nout
         bool first = true;
         int emax = 0;
         for (const Variant &v : kVariants) {
-            if (v.warps == v0.warps && v.psplit == v0.psplit) {
+            if (v.warps == v0.warps && v.psplit == v0.psplit && v.small == small) {
                 emax = std::max(emax, v.ereg);
                 if (&v < &v0)
                     first = false;
@@ -758,29 +870,23 @@ int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdP
             const int need = (nout + G * nblk - 1) / (G * nblk);
             int ereg = 0;
             for (const Variant &v : kVariants)
-                if (v.warps == v0.warps && v.psplit == v0.psplit && v.ereg >= need &&
-                    (ereg == 0 || v.ereg < ereg))
+                if (v.warps == v0.warps && v.psplit == v0.psplit && v.small == small &&
+                    v.ereg >= need && (ereg == 0 || v.ereg < ereg))
                     ereg = v.ereg;
             if (ereg == 0)
                 continue;
             MuladdPlan p;
             p.warps = v0.warps;
             p.psplit = v0.psplit;
+            p.small = small;
             p.ereg = ereg;
             p.nblk = nblk;
-            for (int ns : {1, 2, 3, 4, 6, 8}) {
+            for (int ns : {1, 2, 3, 4, 6, 8, 12, 16}) {
                 p.nsplit = ns;
                 const long long ctas = static_cast<long long>(T) * nblk * ns;
                 if (ns > 1 && (nin / ns < 8 || ctas > 8LL * sms))
                     continue;
-                if (!plan_valid(p, nin, nout, S))
-                    continue;
-                bool dup = false;
-                for (const MuladdPlan &q : cands)
-                    dup = dup || (q.warps == p.warps && q.ereg == p.ereg && q.nblk == p.nblk &&
-                                  q.nsplit == p.nsplit && q.psplit == p.psplit);
-                if (!dup)
-                    cands.push_back(p);
+                add(p);
             }
         }
     }
@@ -888,7 +994,7 @@ __global__ void batch_records_kernel(const RecProb *__restrict__ probs, int np,
         else
             c = gexp[static_cast<uint32_t>((static_cast<uint64_t>(glog[base]) * e) % 65535u)];
     }
-    put_record(p.recs, local, c);
+    write_record(p.recs, local, c, false);  // the batch kernel reads the 8 + 8 form
 }
 
 __global__ void batch_zero_kernel(uint8_t *const *__restrict__ ptrs,
@@ -1026,7 +1132,7 @@ int muladd_run_fixed(cudaStream_t stream, int sm_count, const uint8_t *const *d_
     slices_to_planes<<<static_cast<unsigned>((groups + 255) / 256), 256, 0, stream>>>(
         d_src, nin, T, S, d_planes);
     P2G_CUDA(cudaGetLastError());
-    KernelFn fn = kernel_for(p.warps, p.ereg, p.psplit);
+    KernelFn fn = kernel_for(p);
     size_t smem = smem_bytes(p);
     P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));

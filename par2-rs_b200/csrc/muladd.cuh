@@ -1,13 +1,28 @@
 // muladd.cuh -- host launchers of the GF(2^16) region multiply-accumulate.
 #pragma once
+#include "bitslice.cuh"
 #include "common.cuh"
 
 namespace p2g {
 
+// Problems of at most this many outputs use the small-output tables (6 + 5 +
+// 5 planes: 128 table rows per input instead of 512, 48 row reads per
+// coefficient instead of 32; cheaper below ~24 outputs) and 24-word records;
+// larger ones the 8 + 8 tables and 16-word records.  The form follows from
+// the output count alone, so records built for a problem always match the
+// kernel that reads them.
+constexpr int kSmallOutputs = 24;
+inline int record_words(int nout) { return nout <= kSmallOutputs ? kRecordWordsSmall : kRecordWords; }
+// Bytes of the records of an nin x nout problem.
+inline size_t record_bytes(size_t nin, int nout)
+{
+    return nin * static_cast<size_t>(nout) * record_words(nout) * 4;
+}
+
 // One multiply-accumulate problem of a batch (device-resident description).
 struct BatchProb {
     const uint32_t *planes;  // [nin][T][512]
-    const uint32_t *recs;    // [nin][nout][16]
+    const uint32_t *recs;    // [nin][nout][16] (the batch kernel uses the 8 + 8 tables)
     uint8_t *const *dst;     // nout device pointers
     size_t S;                // bytes per slice
     int nin, nout, T, nblk, nsplit, mode;
@@ -66,7 +81,7 @@ int muladd_variants(int *warps, int *eregs, int *psplits, int cap);
 int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdPlan *best,
                     float *best_ms, int *tried);
 
-// Coefficient records [nin][nout][16 words] from a row-major matrix
+// Coefficient records [nin][nout][record_words(nout)] from a row-major matrix
 // coeff[nout][nin] (coefficients[dst][src] of galois/region/mod.rs:78-82).
 int records_from_matrix(p2g_ctx *ctx, const uint16_t *d_coeff, int nin, int nout,
                         uint32_t *d_recs);

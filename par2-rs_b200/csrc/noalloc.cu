@@ -133,7 +133,7 @@ extern "C" int p2g_encode_noalloc(void *cuda_stream, const uint8_t *const *src, 
     const size_t off_dst = align256(k * sizeof(void *));
     const size_t off_coef = off_dst + align256(r * sizeof(void *));
     const size_t off_rec = off_coef + align256(k * r * 2);
-    const size_t off_pl = off_rec + align256(k * r * 64);
+    const size_t off_pl = off_rec + align256(record_bytes(k, static_cast<int>(r)));
     const size_t need = off_pl + planes_bytes_fixed(static_cast<int>(k), slice_bytes);
     if (need > P2G_NOALLOC_SCRATCH_BYTES) {
         set_error("p2g_encode_noalloc: k=%zu, r=%zu, slice=%zu bytes needs %zu bytes of scratch; "

@@ -195,6 +195,31 @@ def test_every_tile_shape_matches_oracle(ctx):
             assert np.array_equal(got, want), (W, E, P, nblk, ns)
 
 
+@pytest.mark.parametrize("r", [1, 5, 8, 9, 16, 17, 24, 25])
+def test_small_output_tables_match_oracle(ctx, r):
+    """Up to 24 outputs the kernel uses the 6 + 5 + 5 tables (24-word
+    records); 25 is the first problem on the 8 + 8 tables.  Every compiled
+    small shape (8 warps x 1-3 outputs) that covers r, with and without input
+    splits, in store mode and (through the host pipeline's groups) in
+    accumulate mode, gives the oracle's slices; a ragged last tile included."""
+    rng = np.random.default_rng(400 + r)
+    k, S = 48, 2048 * 3 + 36
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = rng.choice(5000, r, replace=False).astype(np.uint32)
+    want = oracle.encode(src, exps)
+    assert np.array_equal(ctx.encode_array(src, exps), want)
+    if r <= 24:
+        for E in (1, 2, 3):
+            if 8 * E < r:
+                continue
+            for ns in (1, 3, 6):
+                ctx.set_plan(k, r, S, 8, E, 1, ns)
+                assert np.array_equal(ctx.encode_array(src, exps), want), (E, ns)
+    # 256 inputs from host buffers: 4 groups, the later ones accumulated
+    big = rng.integers(0, 256, (256, 4096), dtype=np.uint8)
+    assert np.array_equal(ctx.encode_array(big, exps), oracle.encode(big, exps))
+
+
 def test_autotune_picks_a_correct_plan(ctx):
     rng = np.random.default_rng(32)
     k, S, r = 300, 16384, 37
