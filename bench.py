@@ -48,6 +48,10 @@ WORKLOADS = {
     # for an ncu --set full capture
     "profile_encode": (2048, 128 << 10, 205,
                        "profile_encode: k=2048 x 128 KiB seeded uniform random, r=205"),
+    # a small-output problem (13 outputs: the 6 + 5 + 5 tables) at the
+    # profile size, for ncu
+    "profile_small": (2048, 128 << 10, 13,
+                      "profile_small: k=2048 x 128 KiB seeded uniform random, r=13"),
     # the CPU-runnable plain configuration: 16 MiB, 64 KiB slices, 5 %
     "plain": (256, 64 << 10, 13, "plain: 1 file x 16 MiB, 64 KiB slices, k=256, r=13 (5%)"),
 }
@@ -202,11 +206,9 @@ def run_ours(args, rank, world):
     ctx = par2gpu.Context(local)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
-    src_ptrs = [src_dev[i] for i in range(k)]
-    out_ptrs = [out_dev[e] for e in range(r)]
-
+    # [k, S] / [r, S] tensors: one pointer per row from base + i * stride
     def step_dev():
-        ctx.encode(src_ptrs, S, exps, out_ptrs, device=True)
+        ctx.encode(src_dev, S, exps, out_dev, device=True)
 
     plan = None
     if not args.no_autotune:
