@@ -63,6 +63,33 @@ def test_create_damage_repair(tmp_path, scheme):
 
 
 @pytest.mark.gpu
+def test_slices_and_files_larger_than_the_copy_chunks(tmp_path):
+    """12 MiB slices and files of several 8 MiB copy chunks: the recovery
+    slices are read and uploaded in pieces (two per slice), the recovery
+    buffer and the rebuilt files come back in several chunks written at their
+    offsets; the rebuilt bytes equal the originals."""
+    sizes = [30 * (1 << 20) + 4321, 25 * (1 << 20)]
+    files = make_files(tmp_path, sizes, 23)
+    orig = {p.name: p.read_bytes() for p in files}
+    bs = 12 << 20
+    st = fmt.create(files, tmp_path / "big.par2", block_size=bs, redundancy=50)
+    assert st.data_blocks == 3 + 3 and st.recovery_blocks == 3
+    # a slice in the middle of the first file, the last (ragged) one, and
+    # the second file's first slice
+    b = bytearray(orig["part0.bin"])
+    b[bs + 99] ^= 0xFF
+    b[-1] ^= 1
+    (tmp_path / "part0.bin").write_bytes(bytes(b))
+    c = bytearray(orig["part1.bin"])
+    c[7] ^= 0x10
+    (tmp_path / "part1.bin").write_bytes(bytes(c))
+    n, st = fmt.repair(tmp_path / "big.par2", tmp_path)
+    assert n == 3 and st.files_written == 2
+    for p in files:
+        assert p.read_bytes() == orig[p.name], p.name
+
+
+@pytest.mark.gpu
 def test_insufficient_recovery(tmp_path):
     files = make_files(tmp_path, [1 << 20, 1 << 20], 22)
     fmt.create(files, tmp_path / "s.par2", block_size=65536, redundancy=5)  # 2 slices
