@@ -106,7 +106,11 @@ int p2g_autotune(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes, int 
                  p2g_plan *best);
 
 /* Pins the plan for one shape (P2G_EINVAL if the shape is not compiled or
- * does not cover nout outputs). */
+ * does not cover nout outputs).  Problems of at most 24 outputs run the
+ * small-output kernel (three smaller lookup tables per input), compiled for
+ * 8 warps x 1-3 outputs per group, warps_per_group 1; larger problems the
+ * 8 + 8 table kernel (8 warps x 1-13, 12 warps x 4/6/7/8, 16 warps x 2-5,
+ * and 16 warps x 8/10/12 with warps_per_group 2). */
 int p2g_set_plan(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes,
                  const p2g_plan *plan);
 
