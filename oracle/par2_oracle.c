@@ -1,9 +1,10 @@
 /*
  * par2_oracle.c -- TEST INFRASTRUCTURE ONLY.
  *
- * A plain-C restatement of the par2-rs erasure-coding path, used as the parity
- * checker for the CUDA library (tests/, __graft_entry__.smoke() and the
- * cpu_baseline leg of bench.py).  Nothing in the product links or calls it.
+ * A plain-C restatement of the par2-rs erasure-coding path: the parity
+ * reference the CUDA library's results are compared with (tests/,
+ * __graft_entry__.smoke() and the cpu_baseline leg of bench.py).  Nothing in
+ * the product links or calls it.
  *
  * Parity pinning: the restatement is checked against the QuickPar fixture set
  * bundled with par2-rs (tests/data/testdata*.par2): all 60 recovery slices,

@@ -309,7 +309,7 @@ int p2g_create(int device, p2g_ctx **out)
     cudaDeviceProp prop;
     P2G_CUDA(cudaGetDeviceProperties(&prop, device));
     if (prop.major != 10) {
-        set_error("p2g_create: device %d is sm_%d%d, this build targets sm_100a", device,
+        set_error("p2g_create: device %d is sm_%d%d, the library is compiled for sm_100a", device,
                   prop.major, prop.minor);
         return P2G_ENODEV;
     }
