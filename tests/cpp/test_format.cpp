@@ -7,6 +7,14 @@
 //                                             writes a set (GPU: IFSC + recovery)
 //   test_format repair <file.par2> <dir>      verifies every slice on the GPU and
 //                                             rebuilds damaged files in place
+//   test_format blocksize <bytes...>          calculate_block_size of each total,
+//                                             one per line (host only)
+//   test_format volumes <single|exp> <n> <base>
+//                                             split_into_volumes of exponents 0..n-1:
+//                                             "start end count path" per volume
+//   test_format volname <base> <start> <end> <width>
+//                                             generate_volume_filename
+//   test_format padwidth <max...>             calculate_padding_width of each
 #include <stdio.h>
 
 #include <set>
@@ -212,6 +220,33 @@ int main(int argc, char **argv)
                               argv + 6);
         if (cmd == "repair" && argc >= 4)
             return cmd_repair(argv[2], argv[3]);
+        if (cmd == "volumes" && argc >= 5) {
+            std::vector<uint32_t> exps(std::stoul(argv[3]));
+            for (size_t e = 0; e < exps.size(); ++e)
+                exps[e] = static_cast<uint32_t>(e);
+            const VolumeScheme scheme =
+                std::string(argv[2]) == "single" ? VolumeScheme::Single : VolumeScheme::Exponential;
+            for (const VolumeInfo &v : split_into_volumes(exps, scheme, argv[4]))
+                printf("%u %u %zu %s\n", v.exponent_start, v.exponent_end, v.exponents.size(),
+                       v.path.string().c_str());
+            return 0;
+        }
+        if (cmd == "volname" && argc >= 6) {
+            printf("%s\n", generate_volume_filename(argv[2], std::stoul(argv[3]), std::stoul(argv[4]),
+                                                    std::stoul(argv[5]))
+                                .c_str());
+            return 0;
+        }
+        if (cmd == "padwidth") {
+            for (int i = 2; i < argc; ++i)
+                printf("%zu\n", calculate_padding_width(std::stoul(argv[i])));
+            return 0;
+        }
+        if (cmd == "blocksize") {
+            for (int i = 2; i < argc; ++i)
+                printf("%llu\n", static_cast<unsigned long long>(calculate_block_size(std::stoull(argv[i]))));
+            return 0;
+        }
     } catch (const std::exception &e) {
         fprintf(stderr, "error: %s\n", e.what());
         return 1;

@@ -47,6 +47,55 @@ def packet_headers(buf):
     return out
 
 
+def test_calculate_block_size_matches_reference_tests():
+    """creator.rs:539-585 (test_calculate_block_size): its known answers and
+    its properties -- a multiple of 4, at least 2 KiB, at most 4 MiB up to
+    260 GB of data, never more than 65535 slices -- for the C++ product's
+    calculate_block_size (host only)."""
+    sizes = [0, 1000, 1_000_000, 10_000_000, 100_000_000, 1_000_000_000, 10_000_000_000,
+             260_000_000_000, 500_000_000_000, 2 ** 45 + 3]
+    got = [int(x) for x in run("blocksize", *sizes).stdout.split()]
+    bs = dict(zip(sizes, got))
+    assert bs[0] == 2048 and bs[1_000_000] == 2048
+    assert bs[10_000_000] == 5000 and bs[1_000_000_000] == 500_000
+    for n, b in bs.items():
+        assert b % 4 == 0 and b >= 2048, (n, b)
+        if n <= 260_000_000_000:
+            assert b <= 4 * 1024 * 1024, (n, b)
+        if n:
+            assert -(-n // b) <= 65535, (n, b)
+
+
+def test_volume_rules_match_reference_tests():
+    """volumes.rs:214-367: padding widths, volume file names, the Single and
+    Exponential splits (1, 2, 4, ... slices per file), padding by the largest
+    exponent, no volume for no recovery slices, the parent directory kept
+    (host only)."""
+    assert run("padwidth", 0, 9, 10, 99, 100, 999, 1000).stdout.split() == \
+        ["1", "1", "2", "2", "3", "3", "4"]
+    names = [("test", 0, 0, 1, "test.vol0+1.par2"), ("test", 0, 1, 1, "test.vol0+2.par2"),
+             ("test", 0, 9, 2, "test.vol00+10.par2"), ("test", 10, 19, 2, "test.vol10+10.par2"),
+             ("archive", 0, 99, 3, "archive.vol000+100.par2")]
+    for base, a, b, w, want in names:
+        assert run("volname", base, a, b, w).stdout.strip() == want
+
+    def vols(scheme, n, base):
+        out = run("volumes", scheme, n, base).stdout.splitlines()
+        return [(int(a), int(b), int(c), p) for a, b, c, p in (line.split(" ", 3) for line in out)]
+
+    v = vols("single", 3, "test")
+    assert len(v) == 1 and v[0][:3] == (0, 2, 3) and v[0][3].endswith("vol0+3.par2")
+    v = vols("exp", 7, "test")
+    assert [x[:3] for x in v] == [(0, 0, 1), (1, 2, 2), (3, 6, 4)]
+    assert [os.path.basename(x[3]) for x in v] == \
+        ["test.vol0+1.par2", "test.vol1+2.par2", "test.vol3+4.par2"]
+    for _, _, _, p in vols("exp", 100, "test"):
+        assert len(os.path.basename(p)[len("test.vol"):].split("+")[0]) == 2, p
+    assert vols("single", 0, "test") == []
+    v = vols("single", 1, "/some/dir/test")
+    assert len(v) == 1 and v[0][3].startswith("/some/dir/") and "test.vol" in v[0][3]
+
+
 @pytest.fixture
 def qp(tmp_path):
     q = quickpar.load()

@@ -137,6 +137,10 @@ def test_creator_rules():
     # creator.rs:540-585 style checks of the block-size rule
     assert o.calculate_block_size(0) == 2048
     assert o.calculate_block_size(1000) == 2048
+    # creator.rs:541-544
+    assert o.calculate_block_size(1_000_000) == 2048
+    assert o.calculate_block_size(10_000_000) == 5000
+    assert o.calculate_block_size(1_000_000_000) == 500_000
     assert o.calculate_block_size(2000 * 8192) == 8192
     assert o.calculate_block_size(10 ** 12) % 4 == 0
     bs = o.calculate_block_size(10 ** 13)
