@@ -15,6 +15,7 @@
 //   test_format volname <base> <start> <end> <width>
 //                                             generate_volume_filename
 //   test_format padwidth <max...>             calculate_padding_width of each
+//   test_format idless <hexA> <hexB>          file_id_less(A, B) as 1 / 0
 #include <stdio.h>
 
 #include <set>
@@ -235,6 +236,15 @@ int main(int argc, char **argv)
             printf("%s\n", generate_volume_filename(argv[2], std::stoul(argv[3]), std::stoul(argv[4]),
                                                     std::stoul(argv[5]))
                                 .c_str());
+            return 0;
+        }
+        if (cmd == "idless" && argc >= 4) {
+            FileHash a{}, b{};
+            for (int i = 0; i < 16; ++i) {
+                a[i] = static_cast<uint8_t>(std::stoul(std::string(argv[2] + 2 * i, 2), nullptr, 16));
+                b[i] = static_cast<uint8_t>(std::stoul(std::string(argv[3] + 2 * i, 2), nullptr, 16));
+            }
+            printf("%d\n", file_id_less(a, b) ? 1 : 0);
             return 0;
         }
         if (cmd == "padwidth") {

@@ -118,6 +118,28 @@ def test_parse_quickpar_set(qp):
     assert all(rec[e] == q.recovery_md5[e] for e in rec)
 
 
+def test_file_id_order_is_little_endian():
+    """parser.rs:892-902: IDs compare from byte 15 down (par2cmdline's
+    little-endian order), so a high last byte outranks a high first byte."""
+    a = "ff" + "00" * 15
+    b = "00" * 15 + "01"
+    assert run("idless", a, b).stdout.strip() == "1"
+    assert run("idless", b, a).stdout.strip() == "0"
+    assert run("idless", a, a).stdout.strip() == "0"
+
+
+def test_parse_from_a_volume_deduplicates_file_descriptions(qp):
+    """parser.rs:921-954: a volume file repeats every FileDesc packet (vol31+29
+    carries each of the 10 five times); loading the set from it yields one
+    entry per file, in the Main packet's order, with all 60 recovery slices."""
+    q, d = qp
+    p = json.loads(run("parse", d / "testdata.vol31+29.par2").stdout)
+    ids = [f["file_id"] for f in p["files"]]
+    assert len(ids) == 10 and len(set(ids)) == 10
+    assert [f["name"] for f in p["files"]] == [f["name"] for f in q.files]
+    assert sorted(e for e, _ in p["recovery"]) == list(range(60))
+
+
 def test_parser_skips_corrupt_packets_and_garbage(qp):
     q, d = qp
     buf = bytearray(open(d / "testdata.par2", "rb").read())
