@@ -180,3 +180,109 @@ def test_cancel_after_commit_skips_purge(tmp_path):
     for p in files:                               # the repair was committed
         assert p.read_bytes() == orig[p.name]
     assert (tmp_path / "set.par2").exists()       # but the purge was skipped
+
+
+# ---- the reference's edge-case, error-path and robustness tests
+# (tests/edge_cases.rs, tests/error_paths.rs, tests/robustness.rs) -------------
+
+def test_block_size_below_minimum_rejected(tmp_path):
+    """edge_cases.rs test_block_size_too_small: below 2 KiB is an error (0
+    through this C ABI means "choose automatically")."""
+    (tmp_path / "data.bin").write_bytes(b"DATA" * 2500)
+    for bs in (4, 2044):
+        with pytest.raises(fmt.Par2FormatError) as ei:
+            fmt.create([tmp_path / "data.bin"], block_size=bs)
+        assert "at least 2048" in str(ei.value)
+
+
+@pytest.mark.parametrize("content", [b"", b"PAR2\x00PKT", b"\x00" * 4096])
+def test_empty_truncated_and_garbage_par2_files(tmp_path, content):
+    """error_paths.rs test_empty_par2_file / test_truncated_par2_file and
+    edge_cases.rs test_invalid_par2_file: no set is read from them."""
+    p = tmp_path / "bad.par2"
+    p.write_bytes(content)
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair(p, tmp_path)
+    assert ei.value.code == fmt.ERROR
+
+
+@pytest.mark.gpu
+def test_zero_redundancy(tmp_path):
+    """edge_cases.rs test_zero_redundancy: a set with no recovery slices
+    verifies intact files and cannot repair damage."""
+    files = make_files(tmp_path, [5000 * 4], 24)
+    st = fmt.create(files, tmp_path / "z.par2", redundancy=0)
+    assert st.recovery_blocks == 0 and (tmp_path / "z.par2").exists()
+    n, st = fmt.repair(tmp_path / "z.par2", tmp_path)
+    assert n == 0 and st.damaged_blocks == 0
+    b = bytearray(files[0].read_bytes())
+    b[100:200] = b"\xff" * 100
+    files[0].write_bytes(bytes(b))
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair_ex(tmp_path / "z.par2", tmp_path, do_repair=False)
+    assert ei.value.code == fmt.EDAMAGED
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair(tmp_path / "z.par2", tmp_path)
+    assert ei.value.code == fmt.EINSUFFICIENT
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("change", ["truncate", "extend"])
+def test_truncated_and_extended_files(tmp_path, change):
+    """edge_cases.rs test_truncated_file_detection / test_extended_file_
+    detection: verification reports the file damaged; repair restores its
+    exact length and bytes."""
+    files = make_files(tmp_path, [10000 * 8], 25)
+    orig = files[0].read_bytes()
+    # 40 slices of 2 KiB, 24 recovery slices: the cut at 40000 bytes loses 21
+    fmt.create(files, tmp_path / "t.par2", redundancy=60)
+    files[0].write_bytes(orig[:40000] if change == "truncate" else orig + b"EXTRA_DATA")
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair_ex(tmp_path / "t.par2", tmp_path, do_repair=False)
+    assert ei.value.code == fmt.EDAMAGED
+    n, st = fmt.repair(tmp_path / "t.par2", tmp_path)
+    assert n >= 1
+    assert files[0].read_bytes() == orig
+
+
+@pytest.mark.gpu
+def test_all_files_missing(tmp_path):
+    """edge_cases.rs test_all_files_missing: with as many recovery slices as
+    data slices, every file is recreated from the recovery slices alone."""
+    files = make_files(tmp_path, [9000, 70000, 3], 26)
+    orig = {p.name: p.read_bytes() for p in files}
+    st = fmt.create(files, tmp_path / "all.par2", block_size=4096, redundancy=100)
+    assert st.recovery_blocks >= st.data_blocks
+    for p in files:
+        os.unlink(p)
+    n, st = fmt.repair(tmp_path / "all.par2", tmp_path)
+    assert n == st.data_blocks and st.files_written == 3
+    for p in files:
+        assert p.read_bytes() == orig[p.name]
+
+
+@pytest.mark.gpu
+def test_many_small_files_and_monotonic_progress(tmp_path):
+    """robustness.rs test_many_small_files_50, test_progress_never_exceeds_
+    total and test_progress_monotonic_per_operation: 50 small files of mixed
+    sizes, a few damaged; progress stays within its total and never goes
+    back within an operation."""
+    rng = np.random.default_rng(27)
+    files = make_files(tmp_path, [int(x) for x in rng.integers(0, 20000, 50)], 27)
+    orig = {p.name: p.read_bytes() for p in files}
+    fmt.create(files, tmp_path / "many.par2", block_size=2048, redundancy=20)
+    for i in (3, 17, 41):
+        if orig[files[i].name]:
+            b = bytearray(orig[files[i].name])
+            b[len(b) // 2] ^= 0xA5
+            files[i].write_bytes(bytes(b))
+    seen = []
+    n, st = fmt.repair_ex(tmp_path / "many.par2", tmp_path,
+                          progress=lambda op, c, t: seen.append((op, c, t)))
+    for p in files:
+        assert p.read_bytes() == orig[p.name], p.name
+    last = {}
+    for op, c, t in seen:
+        assert 0 <= c <= t, (op, c, t)
+        assert c >= last.get(op, 0), (op, c, last)
+        last[op] = c
