@@ -374,6 +374,24 @@ template <class Fill> void fill_device(size_t n, Fill fill)
             throw Par2Error(e);
 }
 
+// MD5 of n bytes of device memory, copied down in order through one pooled
+// pinned chunk (whole-file hashes are one serial chain).
+inline FileHash md5_of_device(const uint8_t *d, size_t n)
+{
+    uint8_t *buf = PinnedPool::get().take();
+    Md5 h;
+    cudaError_t e = cudaSuccess;
+    for (size_t off = 0; off < n && e == cudaSuccess; off += kPinnedChunk) {
+        const size_t len = std::min(kPinnedChunk, n - off);
+        e = cudaMemcpy(buf, d + off, len, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            h.update(buf, len);
+    }
+    PinnedPool::get().give(buf);
+    cuda_check(e, "cudaMemcpy (file hash)");
+    return h.finalize();
+}
+
 // Copies n bytes of device memory into host memory h (any, pageable).
 inline void copy_to_host(uint8_t *h, const uint8_t *d, size_t n)
 {
@@ -719,7 +737,15 @@ class Par2Repairer {
         stats_.recovery_blocks = p.recovery_blocks.size();
         stats_.ms_scan = ms_since(t0);
         check_cancel();
-        // the files into device slices (no hashing: the slices are verified)
+        // Files whose IFSC entries cover every slice are verified slice by
+        // slice on the device; the others by their whole-file MD5, computed
+        // while they are read (the full-file fallback of verify.rs:522-540).
+        std::vector<char> has_ifsc(p.files_in_order.size(), 0);
+        for (size_t i = 0; i < p.files_in_order.size(); ++i) {
+            const auto it = p.slice_checksums.find(p.files_in_order[i].file_id);
+            has_ifsc[i] = it != p.slice_checksums.end() && it->second.size() >= nblk[i];
+        }
+        // the files into device slices
         const auto t1 = std::chrono::steady_clock::now();
         report(Par2Operation::Verifying, 0, 100);
         codec_ctx();
@@ -729,7 +755,7 @@ class Par2Repairer {
             jobs[i].path = dir_ / p.files_in_order[i].name;
             jobs[i].dst = k ? dev.slice(first[i]) : nullptr;
             jobs[i].length = p.files_in_order[i].length;
-            jobs[i].hash = false;
+            jobs[i].hash = !has_ifsc[i];
         }
         stats_.bytes_read = detail::ingest(jobs, detail::reader_threads(jobs.size()), &cancel_);
         check_cancel();
@@ -741,23 +767,25 @@ class Par2Repairer {
         std::vector<uint32_t> crc(k, 0);
         if (k) {
             std::vector<uint8_t> ok(k, 0);
-            std::vector<bool> listed(k, false);
             for (size_t i = 0; i < p.files_in_order.size(); ++i) {
-                const auto it = p.slice_checksums.find(p.files_in_order[i].file_id);
-                if (it == p.slice_checksums.end())
+                if (!has_ifsc[i])
                     continue;
-                for (uint64_t b = 0; b < nblk[i] && b < it->second.size(); ++b) {
-                    memcpy(md5.data() + (first[i] + b) * 16, it->second[b].md5.data(), 16);
-                    crc[first[i] + b] = it->second[b].crc32;
-                    listed[first[i] + b] = true;
+                const auto &cs = p.slice_checksums.find(p.files_in_order[i].file_id)->second;
+                for (uint64_t b = 0; b < nblk[i]; ++b) {
+                    memcpy(md5.data() + (first[i] + b) * 16, cs[b].md5.data(), 16);
+                    crc[first[i] + b] = cs[b].crc32;
                 }
             }
             std::vector<const uint8_t *> sp = dev.ptrs(0, k);
             check(p2g_verify_slices(codec_ctx(), sp.data(), k, bs, md5.data(), crc.data(), ok.data(),
                                     P2G_DEVICE_PTRS));
-            for (uint64_t g = 0; g < k; ++g)
-                if (!ok[g] || !listed[g])
-                    damaged.push_back(g);
+            for (size_t i = 0; i < p.files_in_order.size(); ++i) {
+                // without IFSC a file is intact or, as a whole, damaged
+                const bool file_ok = !has_ifsc[i] && jobs[i].ok && jobs[i].md5 == p.files_in_order[i].hash;
+                for (uint64_t b = 0; b < nblk[i]; ++b)
+                    if (has_ifsc[i] ? !ok[first[i] + b] : !file_ok)
+                        damaged.push_back(first[i] + b);
+            }
         }
         // a file longer than its FileDesc length: its last slice is rebuilt so
         // that the file is rewritten at its length
@@ -825,22 +853,39 @@ class Par2Repairer {
         // device-to-device copies return before they finish; the check below
         // runs on the codec context's own stream
         detail::cuda_check(cudaStreamSynchronize(cudaStreamLegacy), "cudaStreamSynchronize");
-        // the rebuilt slices against their IFSC entries (the post-repair
-        // verification of lib.rs:302-325, per slice)
+        // the rebuilt slices against their IFSC entries, and files without
+        // them by their whole-file MD5 (the post-repair verification of
+        // lib.rs:302-325)
         {
-            std::vector<uint8_t> wmd5(m * 16), ok(m, 0);
-            std::vector<uint32_t> wcrc(m);
-            std::vector<const uint8_t *> rp2(m);
-            for (uint64_t q = 0; q < m; ++q) {
-                memcpy(wmd5.data() + q * 16, md5.data() + damaged[q] * 16, 16);
-                wcrc[q] = crc[damaged[q]];
-                rp2[q] = dev.slice(damaged[q]);
+            std::vector<uint64_t> slices;  // rebuilt slices of files with IFSC
+            std::set<size_t> whole;        // touched files without
+            size_t fi = 0;
+            for (uint64_t g : damaged) {
+                while (g >= first[fi] + nblk[fi])
+                    ++fi;
+                if (has_ifsc[fi])
+                    slices.push_back(g);
+                else
+                    whole.insert(fi);
             }
-            check(p2g_verify_slices(codec_ctx(), rp2.data(), m, bs, wmd5.data(), wcrc.data(), ok.data(),
-                                    P2G_DEVICE_PTRS));
-            for (uint64_t q = 0; q < m; ++q)
-                if (!ok[q])
-                    throw Par2Error("Repair completed but verification failed - files may still be damaged");
+            const size_t n = slices.size();
+            std::vector<uint8_t> wmd5(n * 16), ok(n, 0);
+            std::vector<uint32_t> wcrc(n);
+            std::vector<const uint8_t *> rp2(n);
+            for (size_t q = 0; q < n; ++q) {
+                memcpy(wmd5.data() + q * 16, md5.data() + slices[q] * 16, 16);
+                wcrc[q] = crc[slices[q]];
+                rp2[q] = dev.slice(slices[q]);
+            }
+            if (n)
+                check(p2g_verify_slices(codec_ctx(), rp2.data(), n, bs, wmd5.data(), wcrc.data(),
+                                        ok.data(), P2G_DEVICE_PTRS));
+            bool good = std::all_of(ok.begin(), ok.end(), [](uint8_t v) { return v != 0; });
+            for (size_t i : whole)
+                good = good && detail::md5_of_device(dev.slice(first[i]), p.files_in_order[i].length) ==
+                                   p.files_in_order[i].hash;
+            if (!good)
+                throw Par2Error("Repair completed but verification failed - files may still be damaged");
         }
         stats_.ms_gpu += ms_since(t3);
         // write every touched file to <name>.par2tmp, then commit them all

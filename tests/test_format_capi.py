@@ -286,3 +286,76 @@ def test_many_small_files_and_monotonic_progress(tmp_path):
         assert 0 <= c <= t, (op, c, t)
         assert c >= last.get(op, 0), (op, c, last)
         last[op] = c
+
+
+def _strip_ifsc(directory, only_file_id=None):
+    """Drops the IFSC packets (all, or those of one File ID) from every .par2
+    file of a set, as a set made without slice checksums would be."""
+    import struct
+
+    for p in directory.iterdir():
+        if p.suffix != ".par2":
+            continue
+        buf, out, pos = p.read_bytes(), bytearray(), 0
+        while pos + 64 <= len(buf):
+            (n,) = struct.unpack_from("<Q", buf, pos + 8)
+            pkt = buf[pos:pos + n]
+            is_ifsc = pkt[48:64] == b"PAR 2.0\x00IFSC\x00\x00\x00\x00"
+            if not (is_ifsc and (only_file_id is None or pkt[64:80] == only_file_id)):
+                out += pkt
+            pos += n
+        p.write_bytes(bytes(out))
+
+
+def _file_ids(par2_path):
+    """File ID of every FileDesc packet, by file name."""
+    import struct
+
+    buf, pos, ids = par2_path.read_bytes(), 0, {}
+    while pos + 64 <= len(buf):
+        (n,) = struct.unpack_from("<Q", buf, pos + 8)
+        if buf[pos + 48:pos + 64] == b"PAR 2.0\x00FileDesc":
+            body = buf[pos + 64:pos + n]
+            ids[body[56:].split(b"\x00")[0].decode()] = body[:16]
+        pos += n
+    return ids
+
+
+@pytest.mark.gpu
+def test_sets_without_ifsc_fall_back_to_whole_file_md5(tmp_path):
+    """verify.rs test_verification_without_ifsc(_detects_damage): with no IFSC
+    packets an intact set verifies by the files' MD5s, and a damaged file is
+    detected and rebuilt as a whole (no slice-level information)."""
+    files = make_files(tmp_path, [10 * 2048 - 7, 40 * 2048], 28)
+    orig = {p.name: p.read_bytes() for p in files}
+    fmt.create(files, tmp_path / "n.par2", block_size=2048, redundancy=30)  # 15 slices
+    _strip_ifsc(tmp_path)
+    n, st = fmt.repair_ex(tmp_path / "n.par2", tmp_path, do_repair=False)
+    assert n == 0 and st.damaged_blocks == 0
+    b = bytearray(orig["part0.bin"])
+    b[5000] ^= 0x01
+    files[0].write_bytes(bytes(b))
+    with pytest.raises(fmt.Par2FormatError) as ei:
+        fmt.repair_ex(tmp_path / "n.par2", tmp_path, do_repair=False)
+    assert ei.value.code == fmt.EDAMAGED
+    n, st = fmt.repair(tmp_path / "n.par2", tmp_path)
+    assert n == 10 and st.files_written == 1          # the whole damaged file
+    for p in files:
+        assert p.read_bytes() == orig[p.name], p.name
+
+
+@pytest.mark.gpu
+def test_mixed_ifsc_and_whole_file_verification(tmp_path):
+    """One file without IFSC (checked by MD5), one with it (checked per
+    slice): a single damaged slice of the second is the only one rebuilt."""
+    files = make_files(tmp_path, [6 * 2048, 30 * 2048 + 99], 29)
+    orig = {p.name: p.read_bytes() for p in files}
+    fmt.create(files, tmp_path / "m.par2", block_size=2048, redundancy=20)
+    _strip_ifsc(tmp_path, only_file_id=_file_ids(tmp_path / "m.par2")["part0.bin"])
+    b = bytearray(orig["part1.bin"])
+    b[2048 * 7 + 3] ^= 0x40
+    files[1].write_bytes(bytes(b))
+    n, st = fmt.repair(tmp_path / "m.par2", tmp_path)
+    assert n == 1 and st.files_written == 1
+    for p in files:
+        assert p.read_bytes() == orig[p.name], p.name
