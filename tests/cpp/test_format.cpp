@@ -16,6 +16,7 @@
 //                                             generate_volume_filename
 //   test_format padwidth <max...>             calculate_padding_width of each
 //   test_format idless <hexA> <hexB>          file_id_less(A, B) as 1 / 0
+//   test_format reccount <blocks> <bs> <pct>  recovery_block_count
 #include <stdio.h>
 
 #include <set>
@@ -236,6 +237,11 @@ int main(int argc, char **argv)
             printf("%s\n", generate_volume_filename(argv[2], std::stoul(argv[3]), std::stoul(argv[4]),
                                                     std::stoul(argv[5]))
                                 .c_str());
+            return 0;
+        }
+        if (cmd == "reccount" && argc >= 5) {
+            printf("%llu\n", static_cast<unsigned long long>(recovery_block_count(
+                                  std::stoull(argv[2]), std::stoull(argv[3]), std::stof(argv[4]))));
             return 0;
         }
         if (cmd == "idless" && argc >= 4) {

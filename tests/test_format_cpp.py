@@ -118,6 +118,17 @@ def test_parse_quickpar_set(qp):
     assert all(rec[e] == q.recovery_md5[e] for e in rec)
 
 
+def test_recovery_block_count_matches_reference():
+    """creator.rs:323-327 (floor of data bytes x percent, then a ceiling
+    division by the slice size): 57 % of 7 slices is 4 (tests/verify.rs
+    test_missing_file_recreation_with_volumes), the plain and large
+    configurations' 13 and 205, 0 % gives none, 100 % as many as data."""
+    cases = [((7, 2048, 57), 4), ((256, 65536, 5), 13), ((2048, 1 << 20, 10), 205),
+             ((40, 2048, 0), 0), ((22, 4096, 100), 22), ((53, 65536, 70), 38)]
+    for (k, bs, pct), want in cases:
+        assert run("reccount", k, bs, pct).stdout.strip() == str(want), (k, bs, pct)
+
+
 def test_file_id_order_is_little_endian():
     """parser.rs:892-902: IDs compare from byte 15 down (par2cmdline's
     little-endian order), so a high last byte outranks a high first byte."""
