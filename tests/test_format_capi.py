@@ -359,3 +359,87 @@ def test_mixed_ifsc_and_whole_file_verification(tmp_path):
     assert n == 1 and st.files_written == 1
     for p in files:
         assert p.read_bytes() == orig[p.name], p.name
+
+
+# ---- cancellation on the QuickPar set (tests/info_and_cancel.rs:216-380) ------
+
+def _qp_set(tmp_path):
+    from tests import quickpar
+
+    q = quickpar.load()
+    q.materialize(str(tmp_path))
+    return tmp_path / "testdata.par2"
+
+
+def _data_files(d):
+    return {p.name: p.read_bytes() for p in sorted(d.iterdir()) if p.suffix == ".data"}
+
+
+def _corrupt(d, name, off, n, byte):
+    b = bytearray((d / name).read_bytes())
+    b[off:off + n] = bytes([byte]) * n
+    (d / name).write_bytes(bytes(b))
+
+
+@pytest.mark.gpu
+def test_preset_cancel_leaves_damaged_files_unchanged(tmp_path):
+    """test_repair_cancellation_preset_flag_is_safe and
+    test_verify_cancellation_preset_flag."""
+    import ctypes
+
+    index = _qp_set(tmp_path)
+    for name in ("test-1.data", "test-6.data"):
+        _corrupt(tmp_path, name, 2048, 8192, 0xAB)
+    before = _data_files(tmp_path)
+    for do_repair in (True, False):
+        with pytest.raises(fmt.Par2FormatError) as ei:
+            fmt.repair_ex(index, tmp_path, do_repair=do_repair, purge=True,
+                          cancel=ctypes.c_int32(1))
+        assert ei.value.code == fmt.ECANCELLED
+        assert _data_files(tmp_path) == before
+    assert index.exists()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("delay_us", [0, 50, 500, 5000])
+def test_cancel_from_another_thread(tmp_path, delay_us):
+    """test_repair_cancellation_from_thread_is_safe: whichever stage the flag
+    lands in, the call either reports ECANCELLED with the data files
+    untouched, or completes with the file repaired and no temp file left."""
+    import ctypes
+    import threading
+    import time
+
+    index = _qp_set(tmp_path)
+    orig = _data_files(tmp_path)
+    _corrupt(tmp_path, "test-4.data", 512, 16384, 0xCD)
+    before = _data_files(tmp_path)
+    flag = ctypes.c_int32(0)
+
+    def setter():
+        time.sleep(delay_us * 1e-6)
+        flag.value = 1
+
+    t = threading.Thread(target=setter)
+    t.start()
+    try:
+        fmt.repair_ex(index, tmp_path, cancel=flag)
+        assert _data_files(tmp_path) == orig
+    except fmt.Par2FormatError as e:
+        assert e.code == fmt.ECANCELLED, e
+        assert _data_files(tmp_path) in (before, orig)   # untouched, or committed
+    finally:
+        t.join()
+    assert not [p for p in tmp_path.iterdir() if p.suffix == ".par2tmp"]
+
+
+@pytest.mark.gpu
+def test_unset_cancel_flag_repairs_normally(tmp_path):
+    """test_normal_cancellable_repair_succeeds_with_flag_unset."""
+    import ctypes
+
+    index = _qp_set(tmp_path)
+    orig = _data_files(tmp_path)
+    _corrupt(tmp_path, "test-2.data", 100, 1000, 0x00)
+    n, st = fmt.repair_ex(index, tmp_path, cancel=ctypes.c_int32(0))
+    assert n == 1 and _data_files(tmp_path) == orig
