@@ -722,6 +722,9 @@ class Par2Repairer {
         report(Par2Operation::Loading, 0, 100);
         Par2File p = Par2File::load(par2_);
         report(Par2Operation::Loading, 100, 100);
+        // the files the set names, in slice order (lib.rs:232-241 reports its
+        // directory scan here)
+        report(Par2Operation::Scanning, 0, 100);
         const uint64_t bs = p.block_size;
         std::vector<uint64_t> first, nblk;
         uint64_t k = 0;
@@ -736,6 +739,7 @@ class Par2Repairer {
         stats_.data_blocks = k;
         stats_.recovery_blocks = p.recovery_blocks.size();
         stats_.ms_scan = ms_since(t0);
+        report(Par2Operation::Scanning, 100, 100);
         check_cancel();
         // Files whose IFSC entries cover every slice are verified slice by
         // slice on the device; the others by their whole-file MD5, computed

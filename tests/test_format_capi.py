@@ -443,3 +443,41 @@ def test_unset_cancel_flag_repairs_normally(tmp_path):
     _corrupt(tmp_path, "test-2.data", 100, 1000, 0x00)
     n, st = fmt.repair_ex(index, tmp_path, cancel=ctypes.c_int32(0))
     assert n == 1 and _data_files(tmp_path) == orig
+
+
+# ---- progress (tests/progress.rs) ---------------------------------------------
+
+@pytest.mark.gpu
+def test_progress_operations_of_repair_and_verify(tmp_path):
+    """test_progress_callbacks_during_repair / _verify_only: repair reports
+    Scanning, Loading, Verifying and Repairing with a non-zero total and
+    current <= total; verify-only never reports Repairing."""
+    files = make_files(tmp_path, [50000 * 4], 30)
+    fmt.create(files, tmp_path / "p.par2", redundancy=20)
+    b = bytearray(files[0].read_bytes())
+    b[1000:6000] = b"\xff" * 5000
+    files[0].write_bytes(bytes(b))
+    seen = []
+    fmt.repair_ex(tmp_path / "p.par2", tmp_path, progress=lambda *a: seen.append(a))
+    ops = {op for op, _, _ in seen}
+    assert ops >= {fmt.OP_SCANNING, fmt.OP_LOADING, fmt.OP_VERIFYING, fmt.OP_REPAIRING}
+    assert all(t > 0 and c <= t for _, c, t in seen)
+    seen.clear()
+    fmt.repair_ex(tmp_path / "p.par2", tmp_path, do_repair=False, progress=lambda *a: seen.append(a))
+    ops = {op for op, _, _ in seen}
+    assert ops >= {fmt.OP_SCANNING, fmt.OP_LOADING, fmt.OP_VERIFYING}
+    assert fmt.OP_REPAIRING not in ops
+
+
+@pytest.mark.gpu
+def test_verify_only_with_purge_removes_the_set(tmp_path):
+    """test_progress_callbacks_with_purge: a verify-only run over intact
+    files with purge set removes every .par2 file of the set."""
+    files = make_files(tmp_path, [20000], 31)
+    fmt.create(files, tmp_path / "q.par2", redundancy=10)
+    assert [p for p in tmp_path.iterdir() if p.suffix == ".par2"]
+    seen = []
+    n, st = fmt.repair_ex(tmp_path / "q.par2", tmp_path, do_repair=False, purge=True,
+                          progress=lambda *a: seen.append(a))
+    assert n == 0 and fmt.OP_VERIFYING in {op for op, _, _ in seen}
+    assert not [p for p in tmp_path.iterdir() if p.suffix == ".par2"]
