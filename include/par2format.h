@@ -54,6 +54,15 @@ int p2f_repair(const char *par2_path, const char *dir, uint64_t *rebuilt, p2f_st
 #define P2F_OP_REPAIRING 3
 typedef void (*p2f_progress_fn)(void *user, int operation, uint64_t current, uint64_t total);
 
+/* p2f_create with Par2Creator::with_progress_callback (creator.rs:245-253):
+ * progress, if not NULL, is called on this thread with P2F_OP_REPAIRING
+ * (the reference's name for encoding progress), current = data slices
+ * encoded and total = data slices: 0 before the files are read, total once
+ * the recovery slices exist. */
+int p2f_create_ex(const char *const *inputs, size_t n, const char *output, uint64_t block_size,
+                  float redundancy_percent, int scheme, p2f_progress_fn progress, void *user,
+                  p2f_stats *stats);
+
 /* Par2Repairer::repair_with_callbacks_cancellable (lib.rs:196-351):
  *   do_repair  0: verify only -- any damage returns P2F_EDAMAGED
  *   purge      1: delete the set's .par2 files after a verified or repaired set

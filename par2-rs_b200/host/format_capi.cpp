@@ -47,6 +47,14 @@ extern "C" {
 int p2f_create(const char *const *inputs, size_t n, const char *output, uint64_t block_size,
                float redundancy_percent, int scheme, p2f_stats *stats)
 {
+    return p2f_create_ex(inputs, n, output, block_size, redundancy_percent, scheme, nullptr,
+                         nullptr, stats);
+}
+
+int p2f_create_ex(const char *const *inputs, size_t n, const char *output, uint64_t block_size,
+                  float redundancy_percent, int scheme, p2f_progress_fn progress, void *user,
+                  p2f_stats *stats)
+{
     g_error.clear();
     try {
         if (!inputs && n)
@@ -67,6 +75,10 @@ int p2f_create(const char *const *inputs, size_t n, const char *output, uint64_t
             c.with_output_path(output);
         if (block_size)
             c.with_block_size(block_size);
+        if (progress)
+            c.with_progress([progress, user](par2::Par2Operation op, uint64_t cur, uint64_t tot) {
+                progress(user, static_cast<int>(op), cur, tot);
+            });
         c.create();
         fill(stats, c.stats());
         return P2F_OK;

@@ -439,6 +439,11 @@ template <class F> void parallel_for(size_t n, F fn)
 
 }  // namespace detail
 
+// Par2Operation of lib.rs:76-81 and the progress callback (operation,
+// current, total)
+enum class Par2Operation { Scanning = 0, Loading = 1, Verifying = 2, Repairing = 3 };
+using ProgressCallback = std::function<void(Par2Operation, uint64_t, uint64_t)>;
+
 class Par2Creator {
   public:
     explicit Par2Creator(std::vector<std::filesystem::path> input_files)
@@ -489,6 +494,14 @@ class Par2Creator {
         creator_ = std::move(t);
         return *this;
     }
+    // creator.rs:245-253: encoding progress as (Repairing, slices done, data
+    // slices), called on the creating thread -- 0 before the files stream in,
+    // all of them once the recovery slices exist
+    Par2Creator &with_progress(ProgressCallback cb)
+    {
+        progress_ = std::move(cb);
+        return *this;
+    }
     const PipelineStats &stats() const { return stats_; }
 
     // Writes the index file and the volumes; returns their paths.
@@ -535,6 +548,8 @@ class Par2Creator {
         stats_.data_blocks = k;
         stats_.recovery_blocks = r;
         stats_.ms_scan = ms_since(t0);
+        if (progress_)
+            progress_(Par2Operation::Repairing, 0, k);
         // every file once: whole-file MD5 on the host, slices to the device
         const auto t1 = std::chrono::steady_clock::now();
         codec_ctx();  // the device context exists before the readers start
@@ -576,6 +591,8 @@ class Par2Creator {
             }
         }
         stats_.ms_gpu = ms_since(t2);
+        if (progress_)
+            progress_(Par2Operation::Repairing, k, k);
         // packets shared by every file, then one file per volume (creator.rs:441-521)
         const auto t3 = std::chrono::steady_clock::now();
         std::vector<FileHash> ids;
@@ -661,13 +678,12 @@ class Par2Creator {
     uint64_t block_size_ = 0;
     float percent_ = 5.0f;
     VolumeScheme scheme_ = VolumeScheme::Exponential;
+    ProgressCallback progress_;
     std::string creator_ = kReferenceCreator;
     PipelineStats stats_;
 };
 
 // Par2Operation (lib.rs:76-81) and the progress callback (operation, current, total)
-enum class Par2Operation { Scanning = 0, Loading = 1, Verifying = 2, Repairing = 3 };
-using ProgressCallback = std::function<void(Par2Operation, uint64_t, uint64_t)>;
 
 struct Cancelled : Par2Error {
     Cancelled() : Par2Error("PAR2 operation cancelled") {}

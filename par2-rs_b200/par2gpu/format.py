@@ -28,6 +28,9 @@ class Stats(ctypes.Structure):
 SIGNATURES = [
     ("p2f_create", [ctypes.POINTER(ctypes.c_char_p), ctypes.c_size_t, ctypes.c_char_p,
                     ctypes.c_uint64, ctypes.c_float, ctypes.c_int, ctypes.POINTER(Stats)]),
+    ("p2f_create_ex", [ctypes.POINTER(ctypes.c_char_p), ctypes.c_size_t, ctypes.c_char_p,
+                       ctypes.c_uint64, ctypes.c_float, ctypes.c_int, PROGRESS_FN,
+                       ctypes.c_void_p, ctypes.POINTER(Stats)]),
     ("p2f_repair", [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64),
                     ctypes.POINTER(Stats)]),
     ("p2f_repair_ex", [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, PROGRESS_FN,
@@ -65,12 +68,21 @@ def _check(rc):
         raise Par2FormatError(rc, lib().p2f_last_error().decode())
 
 
-def create(inputs, output=None, block_size=0, redundancy=5.0, scheme=SCHEME_EXPONENTIAL):
-    """Writes the set of `inputs` (paths); returns the call's Stats."""
+def create(inputs, output=None, block_size=0, redundancy=5.0, scheme=SCHEME_EXPONENTIAL,
+           progress=None):
+    """Writes the set of `inputs` (paths); returns the call's Stats.
+    progress(operation, current, total), if given, receives the encoding
+    progress (p2f_create_ex) on this thread."""
     arr = (ctypes.c_char_p * len(inputs))(*[os.fsencode(str(p)) for p in inputs])
     st = Stats()
-    _check(lib().p2f_create(arr, len(inputs), os.fsencode(str(output)) if output else None,
-                            block_size, redundancy, scheme, ctypes.byref(st)))
+    out = os.fsencode(str(output)) if output else None
+    if progress is None:
+        _check(lib().p2f_create(arr, len(inputs), out, block_size, redundancy, scheme,
+                                ctypes.byref(st)))
+    else:
+        cb = PROGRESS_FN(lambda user, op, cur, tot: progress(op, cur, tot))
+        _check(lib().p2f_create_ex(arr, len(inputs), out, block_size, redundancy, scheme, cb,
+                                   None, ctypes.byref(st)))
     return st
 
 

@@ -25,7 +25,8 @@ def test_format_library_exports_every_declared_symbol():
 
     L = ctypes.CDLL(fmt.LIB_PATH)
     names = declared_symbols("p2f")
-    assert {"p2f_create", "p2f_repair", "p2f_last_error"} <= names
+    assert {"p2f_create", "p2f_create_ex", "p2f_repair", "p2f_repair_ex",
+            "p2f_last_error"} <= names
     for n in sorted(names):
         assert hasattr(L, n), f"missing export {n}"
     assert names == {s[0] for s in fmt.SIGNATURES}

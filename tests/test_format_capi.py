@@ -481,3 +481,17 @@ def test_verify_only_with_purge_removes_the_set(tmp_path):
                           progress=lambda *a: seen.append(a))
     assert n == 0 and fmt.OP_VERIFYING in {op for op, _, _ in seen}
     assert not [p for p in tmp_path.iterdir() if p.suffix == ".par2"]
+
+
+@pytest.mark.gpu
+def test_creator_progress_reaches_the_total(tmp_path):
+    """robustness.rs test_creator_progress_callbacks: creation reports
+    encoding progress (as Repairing, the reference's name for it) from 0 to
+    the number of data slices."""
+    files = make_files(tmp_path, [200000], 32)
+    seen = []
+    st = fmt.create(files, tmp_path / "c.par2", redundancy=10,
+                    progress=lambda *a: seen.append(a))
+    enc = [(c, t) for op, c, t in seen if op == fmt.OP_REPAIRING]
+    assert enc and enc[0] == (0, st.data_blocks) and enc[-1] == (st.data_blocks, st.data_blocks)
+    assert all(a[0] <= b[0] for a, b in zip(enc, enc[1:]))
