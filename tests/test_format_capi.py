@@ -495,3 +495,27 @@ def test_creator_progress_reaches_the_total(tmp_path):
     enc = [(c, t) for op, c, t in seen if op == fmt.OP_REPAIRING]
     assert enc and enc[0] == (0, st.data_blocks) and enc[-1] == (st.data_blocks, st.data_blocks)
     assert all(a[0] <= b[0] for a, b in zip(enc, enc[1:]))
+
+
+@pytest.mark.gpu
+def test_quickpar_set_verifies_with_all_volumes(tmp_path):
+    """repair.rs test_parser_loads_multiple_volumes: the intact QuickPar set,
+    index and six volumes, verifies."""
+    index = _qp_set(tmp_path)
+    n, st = fmt.repair_ex(index, tmp_path, do_repair=False)
+    assert n == 0 and st.damaged_blocks == 0 and st.recovery_blocks == 60
+
+
+@pytest.mark.gpu
+def test_repair_from_exponential_volumes(tmp_path):
+    """robustness.rs test_exponential_volumes_many_blocks: 1 MB at 50 % in
+    exponential volumes (several files), 200 KB overwritten, repaired."""
+    files = make_files(tmp_path, [1_000_000], 33)
+    orig = files[0].read_bytes()
+    fmt.create(files, tmp_path / "volumes.par2", redundancy=50, scheme=fmt.SCHEME_EXPONENTIAL)
+    assert len([p for p in tmp_path.iterdir() if p.suffix == ".par2"]) >= 3
+    b = bytearray(orig)
+    b[100_000:300_000] = b"\xff" * 200_000
+    files[0].write_bytes(bytes(b))
+    n, st = fmt.repair(tmp_path / "volumes.par2", tmp_path)
+    assert n > 0 and files[0].read_bytes() == orig
