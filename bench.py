@@ -79,6 +79,18 @@ def probe_int_peak(device):
     return ops.value, sms.value
 
 
+def cpu_model():
+    """The host CPU's model name (from /proc/cpuinfo; None elsewhere)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -176,7 +188,8 @@ def run_reference(args, rank):
         "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16 (GF(2^16))", "data": "synthetic (seeded uniform bytes)",
         "config": {"workload": WORKLOAD, "sample": sample},
-        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads,
+                         "cpu_model": cpu_model(), "kind": "port",
                          "sample": sample,
                          "what": "par2-rs AVX2-Shuffle strategy restated in C (Rust reference "
                                  "not buildable here), reference threading"},
@@ -313,7 +326,8 @@ def run_ours(args, rank, world):
         threads = os.cpu_count() or 1
         gbs, dt, nbytes, rec_sample = cpu_encode_rate(src_host_np, k, S, r, threads)
         dev_sample = out_dev[:, :CPU_SAMPLE_BYTES].cpu().numpy()
-        cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+        cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "cpu_model": cpu_model(),
+               "kind": "port",
                "sample": f"all {k} slices x first {CPU_SAMPLE_BYTES // 1024} KiB columns, r={r}",
                "seconds": dt,
                "what": "par2-rs AVX2-Shuffle strategy restated in C, reference threading",
