@@ -106,10 +106,16 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # running (first sample written) before the caller's timed region
+        for _ in range(100):
+            if os.path.getsize(self.f.name) > 0 or self.proc.poll() is not None:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -242,13 +248,13 @@ def run_ours(args, rank, world):
     # per-step events.
     big = (k + r) * S > (256 << 20)
     flush = None if big else torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    clocks = ClockSampler(local)
+    clocks.start()  # sampling from the warm-up on, through the timed steps
     for _ in range(args.warmup):
         step_dev()
     ctx.set_timing(True)
-    clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize(dev)
-    clocks.start()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
     mul_ms, launches = [], 0
