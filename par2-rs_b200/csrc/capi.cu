@@ -841,6 +841,11 @@ int p2g_reconstruction_matrix(p2g_ctx *ctx, size_t k, const uint64_t *missing, s
     return finish(ctx);
 }
 
+static int repair_passes(p2g_ctx *ctx, size_t m, size_t np, size_t slice_bytes, int groups,
+                         uint8_t *dp, const ParamLayout &L, size_t exps_off,
+                         const uint32_t *exps, uint8_t *const *out,
+                         const std::vector<uint8_t *> &os, bool o_st, bool dev);
+
 int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missing, size_t m,
                const uint8_t *const *present, const uint32_t *exps,
                const uint8_t *const *recovery, uint8_t *const *out, uint32_t flags)
@@ -879,10 +884,14 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
                 cpres.push_back(c[i]);
         }
     }
-    // slices: present data and recovery inputs, outputs
+    // slices: present data and recovery inputs, outputs.  Host present
+    // slices (128 or more) go up in groups on the copy stream instead, while
+    // the inversion and the earlier groups' multiply-accumulate run.
+    const int groups =
+        (!dev && np >= 128) ? static_cast<int>(std::min<size_t>(p2g_ctx::kPipe, np / 64)) : 1;
     std::vector<uint8_t *> ps, os;
     bool p_st = false, o_st = false;
-    P2G_TRY(stage(ctx, ctx->in_copy, present, np, slice_bytes, dev, true, ps, p_st));
+    P2G_TRY(stage(ctx, ctx->in_copy, present, np, slice_bytes, dev, groups == 1, ps, p_st));
     // the right-hand sides start as copies of the recovery slices
     const size_t slot = round16(slice_bytes);
     P2G_TRY(ctx->rhs.ensure(slot * m));
@@ -907,6 +916,38 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
         memcpy(h + L.b_off, cpres.data(), np * 2);
     P2G_TRY(upload_params(ctx, L));
     uint8_t *dp = ctx->params.as<uint8_t>();
+    if (groups > 1) {
+        // after everything already queued on the compute stream (earlier
+        // users of the staging buffers)
+        P2G_CUDA(cudaEventRecord(ctx->pipe_ev[0], ctx->stream));
+        P2G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ev[0], 0));
+        for (int g = 0; g < groups; ++g) {
+            const size_t i0 = np * g / groups, i1 = np * (g + 1) / groups;
+            const int rc = copy_slices(ps.data() + i0, present + i0, i1 - i0, slice_bytes,
+                                       cudaMemcpyHostToDevice, ctx->copy_stream);
+            if (rc != P2G_OK || cudaEventRecord(ctx->pipe_ev[g], ctx->copy_stream) != cudaSuccess) {
+                cudaStreamSynchronize(ctx->copy_stream);
+                if (rc == P2G_OK)
+                    set_error("cudaEventRecord failed");
+                return rc != P2G_OK ? rc : P2G_ECUDA;
+            }
+        }
+    }
+    // every return below waits for the uploads still reading the caller's
+    // present slices
+    const int rc = repair_passes(ctx, m, np, slice_bytes, groups, dp, L, exps_off, exps, out, os,
+                                 o_st, dev);
+    if (groups > 1)
+        cudaStreamSynchronize(ctx->copy_stream);
+    return rc;
+}
+
+// Steps 1-3 of p2g_repair once its slices and parameters are in place.
+static int repair_passes(p2g_ctx *ctx, size_t m, size_t np, size_t slice_bytes, int groups,
+                         uint8_t *dp, const ParamLayout &L, size_t exps_off,
+                         const uint32_t *exps, uint8_t *const *out,
+                         const std::vector<uint8_t *> &os, bool o_st, bool dev)
+{
     const uint32_t *d_exps = reinterpret_cast<const uint32_t *>(dp + exps_off);
     // 1. A^-1 on the device
     P2G_TRY(ctx->inv.ensure(m * m * 2));
@@ -919,15 +960,22 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
         set_error("Singular matrix");
         return P2G_ESINGULAR;
     }
-    // 2. RHS = R ^ V * present
+    // 2. RHS = R ^ V * present (by input groups as their uploads land)
     if (np) {
         P2G_TRY(ctx->recs.ensure(record_bytes(np, static_cast<int>(m))));
         P2G_TRY(records_par2(ctx, reinterpret_cast<const uint16_t *>(dp + L.b_off), d_exps,
                              static_cast<int>(np), static_cast<int>(m), ctx->recs.as<uint32_t>()));
-        P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.src_off),
-                           static_cast<int>(np),
-                           reinterpret_cast<uint8_t *const *>(dp + L.dst_off),
-                           static_cast<int>(m), slice_bytes, ctx->recs.as<uint32_t>(), 1));
+        const uint8_t *const *d_src = reinterpret_cast<const uint8_t *const *>(dp + L.src_off);
+        const size_t rw = static_cast<size_t>(record_words(static_cast<int>(m)));
+        for (int g = 0; g < groups; ++g) {
+            const size_t i0 = np * g / groups, i1 = np * (g + 1) / groups;
+            if (groups > 1)
+                P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
+            P2G_TRY(muladd_run(ctx, d_src + i0, static_cast<int>(i1 - i0),
+                               reinterpret_cast<uint8_t *const *>(dp + L.dst_off),
+                               static_cast<int>(m), slice_bytes,
+                               ctx->recs.as<uint32_t>() + i0 * m * rw, 1));
+        }
     }
     // 3. missing = A^-1 * RHS
     P2G_TRY(ctx->recs2.ensure(record_bytes(m, static_cast<int>(m))));

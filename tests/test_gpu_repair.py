@@ -178,6 +178,46 @@ def test_repair_matches_oracle(ctx, k, S, m):
     assert np.array_equal(got, src[missing])
 
 
+def test_repair_from_host_buffers_in_upload_groups(ctx):
+    """Host present slices (2041 of them, ragged 2050-byte slices) go up in 16
+    groups while the decode matrix forms and the earlier groups accumulate;
+    the rebuilt slices equal the oracle's."""
+    rng = np.random.default_rng(77)
+    k, S, m = 2048, 2050, 7
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(m, dtype=np.uint32)
+    rec = ctx.encode_array(src, exps)
+    missing = np.sort(rng.choice(k, m, replace=False))
+    data = src.copy()
+    data[missing] = 0
+    want, _ = oracle.reconstruct(data, missing, exps, rec)
+    got = ctx.repair_array(data, missing, exps, rec)
+    assert np.array_equal(got, want) and np.array_equal(got, src[missing])
+
+
+def test_singular_repair_while_uploads_are_in_flight(ctx):
+    """Beyond 32768 slices the constants repeat, so losing slices 5 and
+    5 + 32768 leaves a singular matrix: the host-buffer repair (present slices
+    still going up in groups) reports it, and the context then repairs a
+    normal set correctly."""
+    import par2gpu
+
+    k, S = 32780, 64
+    data = np.zeros((k, S), np.uint8)
+    rec = np.zeros((2, S), np.uint8)
+    with pytest.raises(par2gpu.Par2GpuError) as ei:
+        ctx.repair_array(data, [5, 5 + 32768], np.arange(2, dtype=np.uint32), rec)
+    assert ei.value.code == par2gpu.ESINGULAR and "Singular" in par2gpu.last_error()
+    rng = np.random.default_rng(78)
+    src = rng.integers(0, 256, (300, 4096), dtype=np.uint8)
+    exps = np.arange(4, dtype=np.uint32)
+    rec = ctx.encode_array(src, exps)
+    missing = [3, 150, 151, 299]
+    broken = src.copy()
+    broken[missing] = 0
+    assert np.array_equal(ctx.repair_array(broken, missing, exps, rec), src[missing])
+
+
 def test_repair_with_sparse_exponents(ctx):
     rng = np.random.default_rng(77)
     k, S = 64, 4096
