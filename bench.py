@@ -614,33 +614,6 @@ def run_invert(args):
     print(json.dumps(out), flush=True)
 
 
-def run_tensor_alternative(args):
-    """The GF(2) bit-matrix formulation of the 2 GiB encode on the binary
-    tensor cores: every recovery bit is the parity of an AND-popcount over
-    16 k input bits, 16 r x 16 k x S/2 bit-MACs in all.  Reports the measured
-    binary-MMA rate, the encode time that rate allows at best, and the
-    bit-sliced LOP3 kernel's time for the same set."""
-    k, S, r = WORKLOADS["large_encode"][:3]
-    lib = ctypes.CDLL(os.path.join(ROOT, "par2-rs_b200", "lib", "libp2g_probe.so"))
-    rate, ms = ctypes.c_double(), ctypes.c_double()
-    rc = lib.p2g_probe_bmma(0, ctypes.byref(rate), ctypes.byref(ms))
-    if rc != 0:
-        print(json.dumps({"workload": "tensor_alternative", "error": rc}))
-        return
-    bitmacs = 16 * r * 16 * k * (S // 2)
-    tm = (ctypes.c_double * 4)()
-    trc = lib.p2g_probe_tmem(0, ctypes.c_double(1.965e9), tm)
-    print(json.dumps({"workload": "tensor_alternative: GF(2) bit-matrix encode of k=2048 x 1 MiB, "
-                                  "r=205 on binary MMA (mma.sync m16n8k256 b1 and.popc); tensor "
-                                  "memory as a second table store",
-                      "bmma_bit_macs_per_s": rate.value, "probe_ms": ms.value,
-                      "encode_bit_macs": bitmacs,
-                      "encode_ms_at_bmma_peak": bitmacs / rate.value * 1e3,
-                      "table_reads_bytes_per_sm_clock_at_1965MHz": None if trc else {
-                          "tmem_alone": tm[0], "shared_alone": tm[1],
-                          "interleaved_tmem": tm[2], "interleaved_shared": tm[3]}}), flush=True)
-
-
 def run_create_files(args):
     """Create and repair from files (p2f_create / p2f_repair): the large-encode
     set as 4 files x 512 MiB on tmpfs (page cache), 1 MiB slices, 10 %
@@ -1049,7 +1022,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large_encode",
                     choices=sorted(WORKLOADS) + sorted(HASH_WORKLOADS) +
-                    ["verify_repair", "invert", "tensor_alternative", "create_files", "batched",
+                    ["verify_repair", "invert", "create_files", "batched",
                      "serving"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the heuristic tile shape instead of the autotuned one")
@@ -1065,8 +1038,6 @@ def main():
     if args.workload == "invert":
         run_invert(args)
         return
-    if args.workload == "tensor_alternative":
-        run_tensor_alternative(args)
         return
     if args.workload == "create_files":
         run_create_files(args)

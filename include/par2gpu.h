@@ -260,11 +260,14 @@ int p2g_batch_destroy(p2g_batch *batch);
  * counterpart in par2-rs.
  *   - Allocates nothing: its scratch is one static device array of
  *     P2G_NOALLOC_SCRATCH_BYTES on every GPU that loads this library, held
- *     until the process exits.  A problem whose scratch (about k*r*66 bytes
- *     plus k*slice_bytes rounded up to 2 KiB tiles plus the pointer tables)
- *     exceeds it returns P2G_ERANGE.
+ *     until the process exits.  A problem's scratch is about k*r*98 bytes
+ *     when r <= 24 (2-byte coefficient + 96-byte record per pair) or
+ *     k*r*66 bytes when r > 24 (64-byte records), plus k*slice_bytes rounded
+ *     up to 2 KiB tiles, plus the pointer tables; a problem that needs more
+ *     than the array returns P2G_ERANGE.
  *   - src[k] / out[r] are 16-byte aligned DEVICE pointers on the current
- *     device; the pointer arrays and exps are host arrays.
+ *     device; the pointer arrays and exps are host arrays, pinned or not,
+ *     read before the call returns (the caller may reuse them at once).
  *   - The work is enqueued on cuda_stream (a cudaStream_t; NULL is the legacy
  *     default stream) and the call returns without waiting for it;
  *     synchronise the stream before reading the outputs.

@@ -1132,15 +1132,7 @@ int muladd_run_fixed(cudaStream_t stream, int sm_count, const uint8_t *const *d_
     slices_to_planes<<<static_cast<unsigned>((groups + 255) / 256), 256, 0, stream>>>(
         d_src, nin, T, S, d_planes);
     P2G_CUDA(cudaGetLastError());
-    KernelFn fn = kernel_for(p);
-    size_t smem = smem_bytes(p);
-    P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(smem)));
-    long long grid = static_cast<long long>(T) * p.nblk * p.nsplit;
-    fn<<<static_cast<unsigned>(grid), p.warps * 32, smem, stream>>>(
-        d_planes, d_recs, nin, nout, T, p.nblk, p.nsplit, d_dst, S, 0);
-    P2G_CUDA(cudaGetLastError());
-    return P2G_OK;
+    return launch_kernel(stream, p, d_planes, d_recs, nin, nout, T, d_dst, S, 0);
 }
 
 }  // namespace p2g

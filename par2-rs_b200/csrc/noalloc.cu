@@ -159,10 +159,16 @@ extern "C" int p2g_encode_noalloc(void *cuda_stream, const uint8_t *const *src, 
     uint8_t *base = s.scratch;
     std::vector<uint16_t> coef;
     coefficient_matrix(k, exps, r, coef);
-    // From pageable host memory the source is consumed before the call returns.
-    P2G_CUDA(cudaMemcpyAsync(base, src, k * sizeof(void *), cudaMemcpyHostToDevice, stream));
-    P2G_CUDA(cudaMemcpyAsync(base + off_dst, out, r * sizeof(void *), cudaMemcpyHostToDevice,
+    // The caller's pointer tables may be pinned, and a copy from pinned memory
+    // runs after the call returns; copies of them in pageable memory (staged
+    // by the driver before cudaMemcpyAsync returns) leave the caller free to
+    // reuse its tables as soon as the call is back.
+    std::vector<const uint8_t *> src_tab(src, src + k);
+    std::vector<uint8_t *> out_tab(out, out + r);
+    P2G_CUDA(cudaMemcpyAsync(base, src_tab.data(), k * sizeof(void *), cudaMemcpyHostToDevice,
                              stream));
+    P2G_CUDA(cudaMemcpyAsync(base + off_dst, out_tab.data(), r * sizeof(void *),
+                             cudaMemcpyHostToDevice, stream));
     P2G_CUDA(cudaMemcpyAsync(base + off_coef, coef.data(), k * r * 2, cudaMemcpyHostToDevice,
                              stream));
     uint32_t *recs = reinterpret_cast<uint32_t *>(base + off_rec);

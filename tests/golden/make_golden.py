@@ -2,9 +2,9 @@
 fixture set that par2-rs bundles (tests/data/testdata*.par2 and
 tests/data/test-*.data in the par2-rs repository).
 
-Run in a container that has the par2-rs sources mounted:
+Run where the par2-rs sources are available, giving their fixture folder:
 
-    python tests/golden/make_golden.py /root/reference/tests/data
+    python tests/golden/make_golden.py <par2-rs checkout>/tests/data
 
 The output holds, in the canonical input-slice order of the set (the order of
 the Main packet's recovery-set File ID list, as par2-rs parser.rs:522-596
@@ -147,5 +147,6 @@ def main(src_dir, out_path):
 
 
 if __name__ == "__main__":
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests/data"
-    main(src, os.path.join(os.path.dirname(os.path.abspath(__file__)), "quickpar.json"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <par2-rs checkout>/tests/data")
+    main(sys.argv[1], os.path.join(os.path.dirname(os.path.abspath(__file__)), "quickpar.json"))
