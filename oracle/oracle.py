@@ -43,6 +43,7 @@ def lib():
         _o.po_gf_pow.restype = ctypes.c_uint16
         _o.po_gf_pow.argtypes = [ctypes.c_uint16, ctypes.c_uint64]
         _o.po_par2_constants.argtypes = [S, P]
+        _o.po_power_matrix.argtypes = [P, S, P, S, P]
         _o.po_encode.argtypes = [P, S, S, P, S, P]
         _o.po_muladd_region.argtypes = [P, S, P, S, P, S, S]
         _o.po_invert.restype = ctypes.c_int
@@ -95,6 +96,21 @@ def par2_constants(k):
     out = np.zeros(k, np.uint16)
     lib().po_par2_constants(k, _p(out))
     return out
+
+
+def power_matrix(bases, exps):
+    """uint16 [len(exps), len(bases)]: bases[col] ** exps[row] in GF(2^16)."""
+    b = np.ascontiguousarray(bases, np.uint16)
+    e = np.ascontiguousarray(exps, np.uint32)
+    out = np.zeros((len(e), len(b)), np.uint16)
+    lib().po_power_matrix(_p(b), len(b), _p(e), len(e), _p(out))
+    return out
+
+
+def erasure_matrix(k, missing, exps):
+    """A[row][col] = c_{missing[col]}^{exps[row]} with the PAR2 constants of k
+    input slices (par2_rs.rs:346-353)."""
+    return power_matrix(par2_constants(k)[np.asarray(missing)], exps)
 
 
 def encode(src, exps):

@@ -91,6 +91,17 @@ uint16_t po_gf_pow(uint16_t a, uint64_t n)
     return po_exp[l];
 }
 
+/* The erasure matrix of par2_rs.rs:346-353 (and V of :404-412):
+ * out[row][col] = gf_pow(bases[col], exps[row]) for ne rows x nb columns. */
+void po_power_matrix(const uint16_t *bases, size_t nb, const uint32_t *exps, size_t ne,
+                     uint16_t *out)
+{
+    po_init();
+    for (size_t e = 0; e < ne; ++e)
+        for (size_t j = 0; j < nb; ++j)
+            out[e * nb + j] = po_gf_pow(bases[j], exps[e]);
+}
+
 /* par2_rs.rs:64-76 generate_par2_constants: c_i = 2^n for the i-th n >= 1
  * with n not divisible by 3, 5, 17 or 257. */
 void po_par2_constants(size_t k, uint16_t *out)
