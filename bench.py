@@ -14,7 +14,11 @@ multiply-accumulate.  One "step" is one full encode of that set.
           per symbol multiply-accumulate against the LOP3 rate measured on
           this device, plus its HBM side
   cpu_baseline  the reference's CPU strategy (par2-rs AVX2-Shuffle restated
-          in C, all host threads) on a bounded column sample of the same set
+          in C, all host threads) on the whole set, its recovery slices
+          compared with the GPU's byte for byte (gpu_matches_full)
+  repair / batched / serving  the metric's other parts, on the high-slice-
+          count verify + repair set, 256 heterogeneous sets, and Poisson
+          arrivals at 100 / 1000 / 2000 jobs/s (omitted with --no-legs)
 
 ``--impl reference`` times that CPU strategy alone (rank 0) and prints the
 reference line.  Multi-GPU (torchrun): every rank encodes its own set
@@ -57,7 +61,6 @@ WORKLOADS = {
 }
 K_SRC, SLICE, R_REC, WORKLOAD = WORKLOADS["large_encode"]
 SEED = 20261203
-CPU_SAMPLE_BYTES = 48 * 1024  # columns of every slice in the CPU sample
 
 
 def peaks():
@@ -148,16 +151,15 @@ def gen_sources(k, S, seed):
     return rng.integers(0, 256, (k, S), dtype=np.uint8)
 
 
-def cpu_encode_rate(src_host, k, S, r, threads):
-    """The restated par2-rs AVX2 strategy on a column sample of every slice:
-    returns (source GB/s, seconds, sample bytes, recovery sample)."""
+def cpu_encode_rate(src_host, r, threads):
+    """The restated par2-rs AVX2 strategy on the whole set (every slice, every
+    column): returns (source GB/s, seconds, recovery slices)."""
     from oracle import oracle
 
-    sample = np.ascontiguousarray(src_host[:, :CPU_SAMPLE_BYTES])
     t0 = time.perf_counter()
-    rec = oracle.cpu_encode(sample, r, threads)
+    rec = oracle.cpu_encode(src_host, r, threads)
     dt = time.perf_counter() - t0
-    return sample.nbytes / dt / 1e9, dt, sample.nbytes, rec
+    return src_host.nbytes / dt / 1e9, dt, rec
 
 
 def traffic_from_profile():
@@ -175,7 +177,7 @@ def run_reference(args, rank):
         return
     k, S, r = K_SRC, SLICE, R_REC
     threads = os.cpu_count() or 1
-    src = gen_sources(k, CPU_SAMPLE_BYTES, SEED)
+    src = gen_sources(k, S, SEED)
     from oracle import oracle
 
     for _ in range(args.warmup):
@@ -187,13 +189,13 @@ def run_reference(args, rank):
         times.append(time.perf_counter() - t0)
     dt = sum(times) / len(times)
     gbs = src.nbytes / dt / 1e9
-    sample = f"all {k} slices x first {CPU_SAMPLE_BYTES // 1024} KiB columns, r={r}, per step"
+    sample = f"the whole set per step: all {k} slices x {S} bytes, r={r}"
     line = {
         "impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16 (GF(2^16))", "data": "synthetic (seeded uniform bytes)",
-        "config": {"workload": WORKLOAD, "sample": sample},
+        "config": {"workload": WORKLOAD, "k": k, "r": r, "slice_bytes": S, "sample": sample},
         "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads,
                          "cpu_model": cpu_model(), "kind": "port",
                          "sample": sample,
@@ -326,18 +328,29 @@ def run_ours(args, rank, world):
         "traffic": traffic_from_profile() if WORKLOAD == WORKLOADS["large_encode"][3] else None,
     }
 
-    # ---- CPU baseline + bit-exact cross-check on the same column sample ----
+    # ---- CPU baseline + bit-exact cross-check of the whole recovery output ----
     cpu = None
     if rank == 0 and world == 1:
         threads = os.cpu_count() or 1
-        gbs, dt, nbytes, rec_sample = cpu_encode_rate(src_host_np, k, S, r, threads)
-        dev_sample = out_dev[:, :CPU_SAMPLE_BYTES].cpu().numpy()
+        gbs, dt, rec_cpu = cpu_encode_rate(src_host_np, r, threads)
         cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "cpu_model": cpu_model(),
                "kind": "port",
-               "sample": f"all {k} slices x first {CPU_SAMPLE_BYTES // 1024} KiB columns, r={r}",
+               "sample": f"the whole set: all {k} slices x {S} bytes, r={r}",
                "seconds": dt,
                "what": "par2-rs AVX2-Shuffle strategy restated in C, reference threading",
-               "gpu_matches_sample": bool(np.array_equal(dev_sample, rec_sample))}
+               "gpu_matches_full": bool(np.array_equal(out_dev.cpu().numpy(), rec_cpu))}
+        del rec_cpu
+
+    # ---- the drop-in through the unchanged callers: par2-rs's streaming
+    # encoder (batches of 16-128 blocks, recovery batches of 4-8, one strategy
+    # call per pair from worker threads) over the CUDA strategy's shuffle2x
+    # hooks, host buffers in and out ----
+    trait = None
+    if rank == 0 and world == 1 and not args.no_legs and WORKLOAD == WORKLOADS["large_encode"][3]:
+        try:
+            trait = trait_path_leg(src_host_np, r, out_dev.cpu().numpy(), steps=2)
+        except Exception as exc:  # the headline line must still print
+            trait = {"error": f"{type(exc).__name__}: {exc}"}
 
     # ---- the plain configuration's repair leg: r seeded slices zeroed and
     # rebuilt from the r recovery slices just made (device-resident) ----
@@ -378,6 +391,24 @@ def run_ours(args, rank, world):
                               "(decode matrix + multiply-accumulate), L2 flushed between steps"}
     ctx.close()
 
+    # ---- the metric's other parts: repair at the high-slice-count size,
+    # batched sets and served jobs, each bit-exact against its own check ----
+    legs = {}
+    if rank == 0 and world == 1 and not args.no_legs and WORKLOAD == WORKLOADS["large_encode"][3]:
+        del src_dev, out_dev, src_pinned, out_pinned, host_src, host_out
+        if flush is not None:
+            del flush
+        torch.cuda.empty_cache()
+        for key, fn in (("repair", lambda: verify_repair_leg(autotune=False)),
+                        ("batched", batched_leg),
+                        ("serving", lambda: serving_leg((100, 1000, 2000)))):
+            t0 = time.perf_counter()
+            try:
+                legs[key] = fn()
+            except Exception as exc:  # the headline line must still print
+                legs[key] = {"error": f"{type(exc).__name__}: {exc}"}
+            legs[key]["leg_wall_s"] = time.perf_counter() - t0
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
@@ -398,15 +429,46 @@ def run_ours(args, rank, world):
         }
         if repair_leg is not None:
             line["repair"] = repair_leg
+        if trait is not None:
+            line["trait_path"] = trait
+        line.update(legs)
         print(json.dumps(line), flush=True)
 
 
+def trait_path_leg(src_host, r, want, steps=2):
+    """The encode through par2-rs's unchanged streaming-encoder call sequence
+    (p2f_streaming_encode: par2_rs.rs:687-902 restated over the selected
+    strategy, all host threads) from host buffers; wall time of whole calls,
+    best of `steps` after one warm-up, and equality with `want`."""
+    from par2gpu import format as fmt
+
+    threads = os.cpu_count() or 1
+    k, S = src_host.shape
+    got = fmt.streaming_encode(src_host, r, threads=threads)   # warm-up
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        got = fmt.streaming_encode(src_host, r, threads=threads)
+        times.append(time.perf_counter() - t0)
+    dt = min(times)
+    return {"source_gbs": k * S / dt / 1e9, "seconds": dt, "threads": threads,
+            "bit_exact": bool(np.array_equal(got, want)),
+            "what": "StreamingEncoder process_block x k + finalize over the CUDA strategy's "
+                    "shuffle2x hooks (host u16 buffers, batches of 16-128 data blocks x "
+                    "recovery batches of 4-8 from worker threads); wall time of the whole "
+                    "call, copies included"}
+
+
 def run_verify_repair(args):
+    print(json.dumps(verify_repair_leg(autotune=not args.no_autotune)), flush=True)
+
+
+def verify_repair_leg(autotune=True):
     """The high-slice-count verify + repair configuration: 32000 source slices
     of 64 KiB (~2 GiB, 8 files' worth) with 1600 recovery slices; 1600 slices
     damaged (800 zeroed, 800 with 1-64 flipped bytes); per-slice MD5/CRC32
     verification of all 32000, the 1600 x 1600 inversion and the repair, all
-    checked bit-exact against the pristine slices."""
+    checked bit-exact against the pristine slices.  Returns the results."""
     import torch
 
     import par2gpu
@@ -436,7 +498,7 @@ def run_verify_repair(args):
                 best = (t.ms_total, t.ms_kernel)
         return best
 
-    if not args.no_autotune:
+    if autotune:
         # the encode shape and the two repair passes (present -> RHS, RHS -> missing)
         out["plans"] = {f"{a}x{b}": ctx.autotune(a, b, S).as_dict()
                         for a, b in ((k, m), (k - m, m), (m, m))}
@@ -496,7 +558,9 @@ def run_verify_repair(args):
                      "bit_exact": bool(torch.equal(fixed, pristine)),
                      "int_roofline_frac": (2.0 * macs / (tot * 1e-3)) / int_peak if int_peak else None}
     ctx.close()
-    print(json.dumps(out), flush=True)
+    del src, rec, fixed, pristine
+    torch.cuda.empty_cache()
+    return out
 
 
 HASH_WORKLOADS = {
@@ -696,13 +760,11 @@ def run_create_files(args):
         oracle.hash_slices(slices)
         t_ifsc = time.perf_counter() - t0
         r = int(st.recovery_blocks)
-        gbs_enc, _, nbytes, _ = cpu_encode_rate(slices, slices.shape[0], bs, r, threads)
-        t_enc = total / (gbs_enc * 1e9)
+        _, t_enc, _ = cpu_encode_rate(slices, r, threads)
         t_cpu = t_read + t_md5 + t_ifsc + t_enc
         res["cpu_baseline"] = {
             "value": total / t_cpu / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": f"whole files for MD5 and IFSC; encode on the first "
-                      f"{CPU_SAMPLE_BYTES // 1024} KiB of every slice, scaled",
+            "sample": "whole files: MD5, IFSC and the encode of every slice",
             "s_read": t_read, "s_file_md5": t_md5, "s_ifsc": t_ifsc, "s_encode": t_enc}
         print(json.dumps(res), flush=True)
     finally:
@@ -738,10 +800,15 @@ def batched_sets(seed, nsets=256):
 
 
 def run_batched(args):
+    print(json.dumps(batched_leg()), flush=True)
+
+
+def batched_leg():
     """Many independent sets: per-set plain calls (p2g_encode / p2g_repair,
     one set after another) against the batch executor (one persistent kernel
     per phase over all sets' work items, longest first), and the batch's
-    captured CUDA graph replayed.  Jobs/s and makespan; outputs compared."""
+    captured CUDA graph replayed.  Jobs/s and makespan; outputs compared.
+    Returns the results."""
     import torch
 
     import par2gpu
@@ -897,7 +964,9 @@ def run_batched(args):
     if bad:
         out["repair_mismatch_sets"] = bad[:20]
     ctx.close()
-    print(json.dumps(out), flush=True)
+    del sets, graphs
+    torch.cuda.empty_cache()
+    return out
 
 
 def serving_pool(dev, nsets, seed):
@@ -952,9 +1021,14 @@ def make_jobs(pool, nj, rng, ctx):
 
 
 def run_serving(args):
-    """Poisson arrivals at rates 10..2000 jobs/s; continuous batching versus
-    one job at a time on the same GPU and the same arrival times; jobs/s and
-    p50/p95/p99 latency; every job's outputs compared between the two."""
+    print(json.dumps(serving_leg((10, 100, 500, 1000, 2000))), flush=True)
+
+
+def serving_leg(rates):
+    """Poisson arrivals at the given rates (jobs/s); continuous batching
+    versus one job at a time on the same GPU and the same arrival times;
+    jobs/s and p50/p95/p99 latency; every job's outputs compared between the
+    two.  Returns the results."""
     import torch
 
     import par2gpu
@@ -985,7 +1059,7 @@ def run_serving(args):
     del warm
     torch.cuda.synchronize(dev)
     results = []
-    for lam in (10, 100, 500, 1000, 2000):
+    for lam in rates:
         rng = np.random.default_rng(SEED + lam)
         nj = int(min(240, max(120, lam * 1.5)))
         arrivals = np.cumsum(rng.exponential(1.0 / lam, nj))
@@ -1008,10 +1082,13 @@ def run_serving(args):
         del jobs_a, jobs_b
     for c in ctxs:
         c.close()
-    print(json.dumps({"workload": "serving: Poisson arrivals, 40% create / 40% verify / "
-                                  "20% repair, sizes from the batched distribution (48 "
-                                  "device-resident sets), 120 GB admission budget",
-                      "sweep": results}), flush=True)
+    del pool
+    torch.cuda.empty_cache()
+    return {"workload": "serving: Poisson arrivals, 40% create / 40% verify / 20% repair, "
+                        "sizes from the batched distribution (48 device-resident sets), "
+                        "120 GB admission budget",
+            "all_outputs_identical": all(x["outputs_identical"] for x in results),
+            "sweep": results}
 
 
 def main():
@@ -1028,6 +1105,8 @@ def main():
                     help="use the heuristic tile shape instead of the autotuned one")
     ap.add_argument("--quick", action="store_true",
                     help="device-resident timing only (no e2e, roofline probe or CPU baseline)")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="large_encode without the repair / batched / serving parts")
     args = ap.parse_args()
     if args.workload in HASH_WORKLOADS:
         run_hash(args)

@@ -76,6 +76,20 @@ int p2f_repair_ex(const char *par2_path, const char *dir, int do_repair, int pur
                   p2f_progress_fn progress, void *user, const volatile int32_t *cancel,
                   uint64_t *rebuilt, p2f_stats *stats);
 
+/* Recovery slices through par2-rs's streaming encoder path with the callers
+ * unchanged: Par2ReedSolomon::create_streaming_encoder + process_block per
+ * data block + finalize (par2_rs.rs:687-902), restated on the host over the
+ * selected galois strategy (the CUDA strategy, or the one named by
+ * PAR2_SIMD_STRATEGY).  Data blocks are buffered in batches of 16-128 and
+ * each full batch is multiplied into the recovery accumulators by `threads`
+ * worker threads (0: the host's thread count), recovery batches of 4-8 at a
+ * time, one strategy call per (recovery block, data block) pair -- through
+ * the shuffle2x hooks when the strategy supports them, as par2-rs does.
+ *   src[k]  host data blocks of block_size bytes (even)
+ *   out[r]  host buffers receiving the recovery slices, exponents 0..r-1 */
+int p2f_streaming_encode(const uint8_t *const *src, size_t k, size_t block_size, size_t r,
+                         uint8_t *const *out, int threads);
+
 const char *p2f_last_error(void);
 
 #ifdef __cplusplus

@@ -85,8 +85,13 @@ int p2g_last_timing(p2g_ctx *ctx, p2g_timing *out);
  * warps per CTA; warps_per_group warps share one group of outputs_per_group
  * outputs (each holding 16 / warps_per_group of the 16 bit planes); output
  * blocks of (warps / warps_per_group) * outputs_per_group outputs; input
- * splits (partial sums folded with atomic XOR); and the kernel time it
- * measured at (ms, set by p2g_autotune).  No counterpart in par2-rs, whose
+ * splits (partial sums folded with atomic XOR); the kernel time it measured
+ * at (ms, set by p2g_autotune); the column tile: 1024 symbols (0 means the
+ * same), or 512 for the paired form, in which each warp accumulates
+ * outputs_per_group outputs (an even number), half a warp per output, and a
+ * CTA builds each input's lookup tables once for up to 208 outputs; and the
+ * inputs a CTA takes between two of its barriers (0 or 1; 2 in the paired
+ * form, which then holds four tables).  No counterpart in par2-rs, whose
  * strategies fix their blocking (avx2.rs:700-701 DEST_BATCH / SRC_BATCH). */
 typedef struct {
     int warps;
@@ -95,6 +100,8 @@ typedef struct {
     int output_blocks;
     int input_splits;
     float ms;
+    int tile_symbols;
+    int inputs_per_stage;
 } p2g_plan;
 
 /* Autotuner: times every compiled tile shape (and output-block / input-split
@@ -110,7 +117,9 @@ int p2g_autotune(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes, int 
  * small-output kernel (three smaller lookup tables per input), compiled for
  * 8 warps x 1-3 outputs per group, warps_per_group 1; larger problems the
  * 8 + 8 table kernel (8 warps x 1-13, 12 warps x 4/6/7/8, 16 warps x 2-5,
- * and 16 warps x 8/10/12 with warps_per_group 2). */
+ * and 16 warps x 8/10/12 with warps_per_group 2) or its paired form
+ * (tile_symbols 512: 8 warps x 14-26 even, 12 warps x 16 outputs per
+ * warp; with inputs_per_stage 2: 8 warps x 14/18/22/26, 12 warps x 16). */
 int p2g_set_plan(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes,
                  const p2g_plan *plan);
 
@@ -137,6 +146,32 @@ int p2g_muladd_region(p2g_ctx *ctx, uint16_t *const *dsts, size_t ndst,
                       const uint16_t *const *srcs, size_t nsrc,
                       const uint16_t *const *coeff_rows, size_t off_u16, size_t len_u16,
                       uint32_t flags);
+
+/* GaloisSimdStrategy's shuffle2x hooks (galois/simd/mod.rs:68-127), which
+ * par2-rs calls around its accumulation loops: prepare_shuffle2x on every
+ * accumulator and buffered source (par2_rs.rs:727-731, :792-800, :503-506,
+ * :540-553), muladd_shuffle2x / muladd_region_shuffle2x inside the loops
+ * (par2_rs.rs:859-864 via galois/mod.rs:328-349; :588-599 via
+ * galois/region/mod.rs:195-242) and finish_shuffle2x before an accumulator
+ * is read (par2_rs.rs:884-888, :610-613).  Between its prepare and its finish
+ * a buffer's contents belong to the strategy: here a device copy holds them
+ * (prepare uploads the buffer and does not modify it), the multiply-
+ * accumulates are recorded and run as multi-output kernel launches -- at a
+ * prepare once about 3 ms of kernel work or 1 GiB of sources is waiting, and
+ * at every finish -- and finish writes the accumulator's result back into the
+ * caller's buffer.  Buffers are identified by their start address and must
+ * cover off + len symbols.  A call whose destination was not prepared runs at
+ * once (after the recorded work), as the interface's default would.  Safe
+ * from many threads at once (the recording calls take no context lock);
+ * recorded work runs on the context's stream. */
+int p2g_supports_shuffle2x(void);
+int p2g_prepare_shuffle2x(p2g_ctx *ctx, uint16_t *data, size_t n);
+int p2g_muladd_shuffle2x(p2g_ctx *ctx, uint16_t *dst, const uint16_t *src, size_t n, uint16_t c);
+int p2g_muladd_region_shuffle2x(p2g_ctx *ctx, uint16_t *const *dsts, size_t ndst,
+                                const uint16_t *const *srcs, size_t nsrc,
+                                const uint16_t *const *coeff_rows, size_t off_u16,
+                                size_t len_u16);
+int p2g_finish_shuffle2x(p2g_ctx *ctx, uint16_t *data, size_t n);
 
 /* PAR2 input-slice constants (par2_rs.rs:64-76 generate_par2_constants):
  * out[i] = 2^n_i, n_i the i-th n >= 1 not divisible by 3, 5, 17 or 257. */

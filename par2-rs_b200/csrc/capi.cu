@@ -378,6 +378,7 @@ int p2g_destroy(p2g_ctx *ctx)
         cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream)
         cudaStreamSynchronize(ctx->own_stream);
+    p2g::deferred_release(ctx);
     ctx->planes.release();
     ctx->recs.release();
     ctx->in_copy.release();
@@ -480,7 +481,8 @@ int p2g_autotune(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes, int 
     int tried = 0;
     P2G_TRY(muladd_autotune(ctx, static_cast<int>(nin), static_cast<int>(nout), slice_bytes,
                             reps, &p, &ms, &tried));
-    *best = p2g_plan{p.warps, p.ereg, p.psplit, p.nblk, p.nsplit, ms};
+    *best = p2g_plan{p.warps, p.paired ? 2 * p.ereg : p.ereg, p.psplit, p.nblk, p.nsplit, ms,
+                     p.paired ? 512 : 1024, p.stage};
     return P2G_OK;
 }
 
@@ -499,11 +501,21 @@ int p2g_set_plan(p2g_ctx *ctx, size_t nin, size_t nout, size_t slice_bytes,
     p.nblk = plan->output_blocks;
     p.nsplit = plan->input_splits;
     p.small = nout <= static_cast<size_t>(p2g::kSmallOutputs);  // the table form follows nout
-    if (nin > 65535 || nout > 65535 ||
+    // 512-symbol tiles: a warp accumulates outputs_per_group outputs, two per
+    // lookup (an even count)
+    p.paired = plan->tile_symbols == 512;
+    if (p.paired)
+        p.ereg = plan->outputs_per_group % 2 ? -1 : plan->outputs_per_group / 2;
+    p.stage = plan->inputs_per_stage == 0 ? 1 : plan->inputs_per_stage;
+    if ((plan->tile_symbols != 0 && plan->tile_symbols != 512 && plan->tile_symbols != 1024) ||
+        nin > 65535 || nout > 65535 ||
         !plan_valid(p, static_cast<int>(nin), static_cast<int>(nout), slice_bytes)) {
         set_error("p2g_set_plan: warps=%d outputs_per_group=%d warps_per_group=%d blocks=%d "
-                  "splits=%d is not a compiled shape covering %zu outputs",
-                  p.warps, p.ereg, p.psplit, p.nblk, p.nsplit, nout);
+                  "splits=%d tile_symbols=%d inputs_per_stage=%d is not a compiled shape "
+                  "covering %zu outputs",
+                  plan->warps, plan->outputs_per_group, plan->warps_per_group,
+                  plan->output_blocks, plan->input_splits, plan->tile_symbols,
+                  plan->inputs_per_stage, nout);
         return P2G_EINVAL;
     }
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -565,7 +577,8 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     if (groups >= 4 && d_staged) {
         const p2g::MuladdPlan tp = p2g::choose_plan(ctx, static_cast<int>(k / groups * kTailGroups),
                                                     static_cast<int>(r), slice_bytes);
-        const double waves = static_cast<double>(tiles) * tp.nblk / p2g::plan_slots(ctx, tp);
+        const double waves = static_cast<double>(p2g::plan_tiles(tp, slice_bytes)) * tp.nblk /
+                             p2g::plan_slots(ctx, tp);
         slabs = static_cast<int>(std::min<double>(kMaxTailSlabs, std::floor(waves + 0.5)));
         if (static_cast<size_t>(slabs) > tiles)
             slabs = 1;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -43,9 +44,14 @@ struct MuladdPlan {
     int nsplit = 1;
     int psplit = 1;  // warps sharing one output group (each holds 16/psplit planes)
     bool small = false;  // small-output tables (set for problems of <= kSmallOutputs outputs)
+    bool paired = false; // 512-symbol tiles, two outputs per warp lookup (more than 104 outputs)
+    int stage = 1;       // inputs per CTA barrier (2: paired form only)
 };
 
 using PlanKey = std::tuple<int, int, size_t>;  // inputs, outputs, slice bytes
+
+// Device mirrors and recorded products of the shuffle2x hooks (deferred.cu).
+struct Deferred;
 inline PlanKey plan_key(int nin, int nout, size_t S) { return PlanKey(nin, nout, S); }
 
 }  // namespace p2g
@@ -106,7 +112,15 @@ struct p2g_ctx {
     // device or pinned memory synchronises the whole device, which would stall
     // a batch being prepared while another one runs.  Guarded by `mu`.
     std::vector<p2g::DevBuf> spare;
+    // the shuffle2x hooks' state, created on first use (read without the
+    // context lock by the recording calls)
+    std::atomic<p2g::Deferred *> deferred{nullptr};
 };
+
+namespace p2g {
+// Frees the shuffle2x state (mirrors, staging, pool) of a context.
+void deferred_release(p2g_ctx *ctx);
+}  // namespace p2g
 
 #define P2G_CUDA(call)                                                                  \
     do {                                                                                \

@@ -49,6 +49,10 @@ constexpr int kTableBytes = kTableWords * 4; // 64 KiB
 constexpr int kSmallTableWords = 128 * 32;   // T0, T1, T2 of the small-output form
 constexpr int kSmallTableBytes = kSmallTableWords * 4;  // 16 KiB
 constexpr int kRing = 4;
+constexpr int kPairTileBytes = 1024;          // 512 symbols (paired form)
+constexpr int kPairTableWords = 256 * 32;     // 256 combined rows of 128 B
+// ring slots of the paired form with one / two inputs per CTA barrier
+__host__ __device__ constexpr int pair_ring_slots(int stage) { return stage == 1 ? 4 : 6; }
 
 // Four 8x8 b16 matrices from shared memory: lanes 8m..8m+7 give the row
 // addresses of matrix m, lane L receives word L % 4 of row L / 4 of each.
@@ -382,12 +386,18 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
                                                          kTileBytes) +
                          my0 * 4 + (lane >> 3);
         const uint32_t tb = tab_s + buf * kTableBytes;
+        // the next output's record is loaded before this output's lookups, so
+        // it does not wait behind them in the shared-memory queue (loads past
+        // the block's last output stay inside the ring slot and go unused)
+        uint4 nxt = R[0];
 #pragma unroll
         for (int e = 0; e < EREG; ++e) {
             if (e < myn) {
                 uint32_t w[4];
                 if constexpr (PSPLIT == 1) {
-                    const uint4 r = R[e * 4];
+                    const uint4 r = nxt;
+                    if (e + 1 < EREG)
+                        nxt = R[(e + 1) * 4];
                     w[0] = r.x;
                     w[1] = r.y;
                     w[2] = r.z;
@@ -487,6 +497,253 @@ __global__ void __launch_bounds__(WARPS * 32, SMALL ? 2 : 1)
                                             dst, S, nsplit > 1 ? 2 : mode);
 }
 
+// The paired form: a CTA owns a column tile of 512 symbols (half of a plane
+// tile) and each warp accumulates TWO outputs per table lookup, lanes 0-15 one
+// and lanes 16-31 the other (lane L owning symbol group L % 16).  Both halves
+// share the input's tables, so one table build serves up to 16 * EREG
+// outputs per warp pair count -- 208 for EREG = 13, which covers r = 205 in
+// one output block where the 1024-symbol form needs two blocks, each
+// building the same tables.  The table build halves with the tile (256
+// combined rows per input instead of 512 rows), the lookups per output do
+// not change.
+//
+// Table: 256 combined rows of 128 bytes, row n = [T0 row n | T1 row n] with
+// T0 row n (words 0-15) the XOR of planes {b < 8 : bit b of n} for groups
+// 0-15 and T1 row n (words 16-31) that of planes {8 + b}.  One ldmatrix.x4
+// serves a plane pair of both outputs: in each of its four 8x8 matrices one
+// half-warp reads a T0 half-row and the other a T1 half-row (64 bytes each,
+// disjoint banks), so every matrix is one conflict-free wavefront:
+//   matrix 0: lanes 0-15 T0[n0_2k(A)], lanes 16-31 T1[n1_2k(B)]
+//   matrix 1: lanes 0-15 T1[n1_2k(A)], lanes 16-31 T0[n0_2k(B)]
+//   matrix 2, 3: the same for plane 2k + 1
+// (A, B: the outputs of the two halves).  Records are the 16-word records of
+// the 1024-symbol form (bitslice.cuh make_record): record word 4m + i holds the
+// class-m offsets, and the lanes that give matrix m's addresses for output B
+// read class m ^ 1, whose T0 / T1 roles are swapped.  A record offset
+// (n + 256 t) * 128 becomes n * 128 + 64 t here.
+template <int WARPS, int EREG, int STAGE>
+__device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t *__restrict__ planes,
+                                                   const uint32_t *__restrict__ recs, int nout,
+                                                   int T, int u, int ob, int i0, int i1,
+                                                   uint8_t *const *__restrict__ dst, size_t S,
+                                                   int smode)
+{
+    static_assert(STAGE == 1 || STAGE == 2, "one or two inputs per barrier");
+    constexpr int THREADS = WARPS * 32;
+    constexpr int EBLK = WARPS * EREG * 2;                 // outputs per block
+    constexpr int TW = kPairTableWords;                    // words per table buffer
+    constexpr int SLOT = kPairTileBytes + EBLK * kRecordWords * 4;
+    constexpr int RING = pair_ring_slots(STAGE);
+    uint32_t *tab = reinterpret_cast<uint32_t *>(smem);
+    uint8_t *ring = smem + 2 * STAGE * TW * 4;
+    // ring slot of input i (RING = 4 needs no reference to i0)
+    auto slot = [&](int i) {
+        return ring + (RING == 4 ? (i & 3) : (i - i0) % RING) * SLOT;
+    };
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int half = lane >> 4;
+    const int grp = lane & 15;
+    const int obase = ob * EBLK;
+    const int nb = min(EBLK, nout - obase);
+    const int npairs = (nb + 1) >> 1;
+    // a partial block's pairs are spread evenly over the warps
+    const int per = (npairs + WARPS - 1) / WARPS;
+    const int q0 = warp * per;
+    const int myq = max(0, min(per, npairs - q0));
+    const int t = u >> 1, hsel = u & 1;  // plane tile and its half
+
+    auto issue = [&](int i) {
+        if (i < i1) {
+            uint8_t *s = slot(i);
+            // planes b = 0..15, groups 16 hsel .. 16 hsel + 15: 64 bytes each
+            const uint8_t *gp = reinterpret_cast<const uint8_t *>(
+                planes + (static_cast<size_t>(i) * T + t) * 512 + hsel * 16);
+            const uint8_t *gr = reinterpret_cast<const uint8_t *>(
+                recs + (static_cast<size_t>(i) * nout + obase) * kRecordWords);
+            const int nchunk = 64 + nb * (kRecordWords / 4);
+            for (int c = threadIdx.x; c < nchunk; c += THREADS) {
+                // plane b goes to position 2 (b % 8) + b / 8, so that planes
+                // b and b + 8, read together by the two halves of a warp in
+                // the build, share one 128-byte row of banks
+                if (c < 64)
+                    cp_async16(s + (((c >> 2) & 7) * 2 + (c >> 5)) * 64 + (c & 3) * 16,
+                               gp + (c >> 2) * 128 + (c & 3) * 16);
+                else
+                    cp_async16(s + kPairTileBytes + (c - 64) * 16, gr + (c - 64) * 16);
+            }
+        }
+        cp_async_commit();
+    };
+
+    // Lane L writes word L of the combined rows: lanes 0-15 T0 (planes 0-7 of
+    // group L), lanes 16-31 T1 (planes 8-15 of group L - 16).  The 256 rows
+    // form 16 groups of 16 (low nibble: planes 0-3 of the half, high nibble
+    // h: planes 4-7); warp w builds groups [16w/WARPS, 16(w+1)/WARPS).
+    auto build = [&](int i, int buf) {
+        const uint32_t *P = reinterpret_cast<const uint32_t *>(slot(i));
+        uint32_t p[8];
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+            p[b] = P[(b * 2 + half) * 16 + grp];
+        uint32_t L[16];
+        L[0] = 0;
+        L[1] = p[0];
+        L[2] = p[1];
+        L[3] = p[0] ^ p[1];
+        L[4] = p[2];
+        L[5] = L[4] ^ p[0];
+        L[6] = L[4] ^ p[1];
+        L[7] = L[6] ^ p[0];
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+            L[8 + x] = L[x] ^ p[3];
+        const int g0 = warp * 16 / WARPS, g1 = (warp + 1) * 16 / WARPS;
+        constexpr int GMAX = (16 + WARPS - 1) / WARPS;
+        uint32_t *Tp = tab + buf * TW + g0 * 16 * 32 + lane;
+#pragma unroll
+        for (int gg = 0; gg < GMAX; ++gg) {
+            if (GMAX * WARPS == 16 || g0 + gg < g1) {
+                const int h = g0 + gg;
+                const uint32_t H = ((h & 1) ? p[4] : 0u) ^ ((h & 2) ? p[5] : 0u) ^
+                                   ((h & 4) ? p[6] : 0u) ^ ((h & 8) ? p[7] : 0u);
+#pragma unroll
+                for (int x = 0; x < 16; ++x)
+                    Tp[(gg * 16 + x) * 32] = H ^ L[x];
+            }
+        }
+    };
+
+    uint32_t acc[EREG][16];
+#pragma unroll
+    for (int e = 0; e < EREG; ++e)
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            acc[e][j] = 0;
+
+    // As an address giver, lane L serves matrix m = L / 8 for output s =
+    // (L / 4) & 1 of the pair (chunk L % 4 of that output's half-row) and
+    // reads record class m ^ s of output s; the last output of an odd block
+    // reads the block's last record instead (its sums are never stored).
+    const int gs = (lane >> 2) & 1;
+    const int gcls = (lane >> 3) ^ gs;
+    const uint32_t tab_s = static_cast<uint32_t>(__cvta_generic_to_shared(tab)) + (lane & 3) * 16;
+    auto consume = [&](int i, int buf) {
+        const uint4 *R = reinterpret_cast<const uint4 *>(slot(i) + kPairTileBytes);
+        const uint32_t tb = tab_s + buf * TW * 4;
+        // the next pair's record is loaded before this pair's lookups
+        uint4 nxt = R[min(2 * q0 + gs, nb - 1) * 4 + gcls];
+#pragma unroll
+        for (int e = 0; e < EREG; ++e) {
+            if (e < myq) {
+                const uint4 r = nxt;
+                if (e + 1 < EREG)
+                    nxt = R[min(2 * (q0 + e + 1) + gs, nb - 1) * 4 + gcls];
+                // (n + 256 t) * 128 -> n * 128 + 64 t, both halves of a word
+                uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    w[q] = (w[q] & 0x7FFF7FFFu) | ((w[q] >> 9) & 0x00400040u);
+#pragma unroll
+                for (int p = 0; p < 8; ++p) {
+                    const uint32_t off = (p & 1) ? (w[p >> 1] >> 16) : (w[p >> 1] & 0xFFFFu);
+                    uint32_t d0, d1, d2, d3;
+                    ldsm_x4(tb + off, d0, d1, d2, d3);
+                    acc[e][2 * p] ^= d0 ^ d1;
+                    acc[e][2 * p + 1] ^= d2 ^ d3;
+                }
+            }
+        }
+    };
+
+    if constexpr (STAGE == 1) {
+        // one input per barrier: build input i + 1 while consuming input i
+        if (i0 < i1) {
+            issue(i0);
+            issue(i0 + 1);
+            issue(i0 + 2);
+            cp_async_wait<1>();
+            __syncthreads();
+            build(i0, 0);
+            __syncthreads();
+            for (int i = i0; i < i1; ++i) {
+                issue(i + 3);
+                if (i + 1 < i1)
+                    build(i + 1, (i + 1 - i0) & 1);
+                consume(i, (i - i0) & 1);
+                cp_async_wait<1>();
+                __syncthreads();
+            }
+        }
+    } else {
+        // two inputs per barrier (four table buffers, six ring slots): stage
+        // s consumes inputs s, s + 1 from one table pair, builds s + 2, s + 3
+        // into the other, and fetches s + 4, s + 5, which land before the
+        // barrier that ends the stage
+        if (i0 < i1) {
+            issue(i0);
+            issue(i0 + 1);
+            issue(i0 + 2);
+            issue(i0 + 3);
+            cp_async_wait<2>();
+            __syncthreads();
+            build(i0, 0);
+            if (i0 + 1 < i1)
+                build(i0 + 1, 1);
+            cp_async_wait<0>();
+            __syncthreads();
+            for (int s = i0; s < i1; s += 2) {
+                const int tp = ((s - i0) >> 1) & 1;
+                issue(s + 4);
+                issue(s + 5);
+                if (s + 2 < i1)
+                    build(s + 2, 2 * (tp ^ 1));
+                if (s + 3 < i1)
+                    build(s + 3, 2 * (tp ^ 1) + 1);
+                consume(s, 2 * tp);
+                if (s + 1 < i1)
+                    consume(s + 1, 2 * tp + 1);
+                cp_async_wait<0>();
+                __syncthreads();
+            }
+        }
+    }
+    cp_async_wait<0>();
+
+#pragma unroll
+    for (int e = 0; e < EREG; ++e) {
+        const int o = 2 * (q0 + e) + half;
+        if (e < myq && o < nb) {
+            uint32_t x[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                x[j] = acc[e][j];
+            transpose16x2(x);
+            store_group(dst[obase + o], S, static_cast<size_t>(u) * kPairTileBytes + grp * 64, x,
+                        smode);
+        }
+    }
+}
+
+template <int WARPS, int EREG, int STAGE>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+    muladd_paired(const uint32_t *__restrict__ planes, const uint32_t *__restrict__ recs,
+                  int nin, int nout, int T, int nblk, int nsplit,
+                  uint8_t *const *__restrict__ dst, size_t S, int mode)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    int bid = blockIdx.x;
+    const int split = bid % nsplit;
+    bid /= nsplit;
+    const int ob = bid % nblk;
+    const int u = bid / nblk;
+    const int i0 = static_cast<int>(static_cast<long long>(nin) * split / nsplit);
+    const int i1 = static_cast<int>(static_cast<long long>(nin) * (split + 1) / nsplit);
+    muladd_item_paired<WARPS, EREG, STAGE>(smem, planes, recs, nout, T, u, ob, i0, i1, dst, S,
+                                           nsplit > 1 ? 2 : mode);
+}
+
 // Persistent form for batches of independent problems: one CTA per SM takes
 // items (problem, tile, output block, input split) from a queue ordered
 // longest first and runs each as muladd_bitsliced would.
@@ -544,15 +801,19 @@ using KernelFn = void (*)(const uint32_t *, const uint32_t *, int, int, int, int
 
 struct Variant {
     int warps, ereg, psplit;
-    bool small;  // small-output tables (problems of at most kSmallOutputs outputs)
+    bool small;   // small-output tables (problems of at most kSmallOutputs outputs)
+    bool paired;  // 512-symbol tiles, two outputs per warp lookup (muladd_paired)
+    int stage;    // inputs per CTA barrier (paired form: 1 or 2)
     KernelFn fn;
 };
 
 // Compiled tile shapes: warps per CTA x outputs per warp.  The register
 // budget (64K per SM, one CTA per SM) caps EREG at 13 / 8 / 5 for 8 / 12 / 16
-// warps without spills.
-#define P2G_V(W, E, P) {W, E, P, false, muladd_bitsliced<W, E, P>}
-#define P2G_VS(E) {8, E, 1, true, muladd_bitsliced<8, E, 1, true>}
+// warps without spills; the paired form holds EREG pairs of outputs per warp
+// (2 x EREG outputs, EREG x 16 accumulator registers per lane).
+#define P2G_V(W, E, P) {W, E, P, false, false, 1, muladd_bitsliced<W, E, P>}
+#define P2G_VS(E) {8, E, 1, true, false, 1, muladd_bitsliced<8, E, 1, true>}
+#define P2G_VP(W, E, G) {W, E, 1, false, true, G, muladd_paired<W, E, G>}
 static const Variant kVariants[] = {
     P2G_VS(1),        P2G_VS(2),        P2G_VS(3),
     P2G_V(8, 1, 1),   P2G_V(8, 2, 1),   P2G_V(8, 3, 1),   P2G_V(8, 4, 1),   P2G_V(8, 5, 1),
@@ -560,20 +821,25 @@ static const Variant kVariants[] = {
     P2G_V(8, 11, 1),  P2G_V(8, 12, 1),  P2G_V(8, 13, 1),  P2G_V(12, 4, 1),  P2G_V(12, 6, 1),
     P2G_V(12, 7, 1),  P2G_V(12, 8, 1),  P2G_V(16, 2, 1),  P2G_V(16, 3, 1),  P2G_V(16, 4, 1),
     P2G_V(16, 5, 1),  P2G_V(16, 8, 2),  P2G_V(16, 10, 2), P2G_V(16, 12, 2),
+    P2G_VP(8, 7, 1),  P2G_VP(8, 8, 1),  P2G_VP(8, 9, 1),  P2G_VP(8, 10, 1), P2G_VP(8, 11, 1),
+    P2G_VP(8, 12, 1), P2G_VP(8, 13, 1), P2G_VP(12, 8, 1), P2G_VP(8, 7, 2),  P2G_VP(8, 9, 2),
+    P2G_VP(8, 11, 2), P2G_VP(8, 13, 2), P2G_VP(12, 8, 2),
 };
 #undef P2G_V
 #undef P2G_VS
+#undef P2G_VP
 
-static KernelFn kernel_for(int warps, int ereg, int psplit, bool small)
+static KernelFn kernel_for(int warps, int ereg, int psplit, bool small, bool paired, int stage)
 {
     for (const Variant &v : kVariants)
-        if (v.warps == warps && v.ereg == ereg && v.psplit == psplit && v.small == small)
+        if (v.warps == warps && v.ereg == ereg && v.psplit == psplit && v.small == small &&
+            v.paired == paired && v.stage == stage)
             return v.fn;
     return nullptr;
 }
 static KernelFn kernel_for(const MuladdPlan &p)
 {
-    return kernel_for(p.warps, p.ereg, p.psplit, p.small);
+    return kernel_for(p.warps, p.ereg, p.psplit, p.small, p.paired, p.stage);
 }
 
 // The 8 + 8 shapes (the small-output form reuses 8-warp shapes of 1-3
@@ -582,7 +848,7 @@ int muladd_variants(int *warps, int *eregs, int *psplits, int cap)
 {
     int n = 0;
     for (const Variant &v : kVariants) {
-        if (v.small)
+        if (v.small || v.paired)
             continue;
         if (n < cap) {
             warps[n] = v.warps;
@@ -595,10 +861,22 @@ int muladd_variants(int *warps, int *eregs, int *psplits, int cap)
 }
 
 // outputs one CTA of this shape covers
-static int block_outputs(const MuladdPlan &p) { return p.warps / p.psplit * p.ereg; }
+static int block_outputs(const MuladdPlan &p)
+{
+    return p.paired ? p.warps * p.ereg * 2 : p.warps / p.psplit * p.ereg;
+}
+
+int plan_tiles(const MuladdPlan &p, size_t S)
+{
+    const size_t tb = p.paired ? kPairTileBytes : kTileBytes;
+    return static_cast<int>((S + tb - 1) / tb);
+}
 
 static size_t smem_bytes(const MuladdPlan &p)
 {
+    if (p.paired)
+        return 2 * p.stage * kPairTableWords * 4 +
+               pair_ring_slots(p.stage) * (kPairTileBytes + block_outputs(p) * kRecordWords * 4);
     if (p.small)
         return 2 * kSmallTableBytes + kRing * (kTileBytes + block_outputs(p) * kRecordWordsSmall * 4);
     return 2 * kTableBytes + kRing * (kTileBytes + block_outputs(p) * kRecordWords * 4);
@@ -609,8 +887,8 @@ static size_t smem_bytes(const MuladdPlan &p)
 static int resident_ctas(const MuladdPlan &p)
 {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, bool>, int> cache;
-    const auto key = std::make_tuple(p.warps, p.ereg, p.psplit, p.small);
+    static std::map<std::tuple<int, int, int, bool, bool, int>, int> cache;
+    const auto key = std::make_tuple(p.warps, p.ereg, p.psplit, p.small, p.paired, p.stage);
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end())
@@ -644,11 +922,21 @@ MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t S)
             return it->second;
     }
     MuladdPlan p;
-    const int T = static_cast<int>((S + kTileBytes - 1) / kTileBytes);
     p.warps = 8;
     p.small = nout <= kSmallOutputs;
-    p.nblk = (nout + 8 * 13 - 1) / (8 * 13);
-    p.ereg = std::max(1, (nout + 8 * p.nblk - 1) / (8 * p.nblk));
+    if (nout > 8 * 13) {
+        // more outputs than one 1024-symbol block holds: the paired form
+        // (up to 208 outputs per block) builds each input's tables half as
+        // often per output
+        p.paired = true;
+        p.nblk = (nout + 8 * 13 * 2 - 1) / (8 * 13 * 2);
+        const int pairs = ((nout + p.nblk - 1) / p.nblk + 1) / 2;
+        p.ereg = std::max(7, (pairs + 7) / 8);
+    } else {
+        p.nblk = (nout + 8 * 13 - 1) / (8 * 13);
+        p.ereg = std::max(1, (nout + 8 * p.nblk - 1) / (8 * p.nblk));
+    }
+    const int T = plan_tiles(p, S);
     // Input splits (atomic-XOR folds, whole aligned words: S % 4 == 0) for
     // grids that would leave SMs idle.  A CTA costs its inputs plus a fixed
     // prologue/epilogue of ~17 input tiles (~20 when it folds atomically),
@@ -678,8 +966,8 @@ MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t S)
 
 bool plan_valid(const MuladdPlan &p, int nin, int nout, size_t S)
 {
-    if (p.psplit < 1 || p.small != (nout <= kSmallOutputs) || kernel_for(p) == nullptr ||
-        p.nblk < 1)
+    if (p.psplit < 1 || p.small != (nout <= kSmallOutputs) || (p.paired && p.small) ||
+        (!p.paired && p.stage != 1) || kernel_for(p) == nullptr || p.nblk < 1)
         return false;
     const long long eb = block_outputs(p);
     return p.nblk * eb >= nout && (p.nblk - 1) * eb < nout && p.nsplit >= 1 &&
@@ -720,7 +1008,8 @@ static int launch_kernel(cudaStream_t stream, const MuladdPlan &p, const uint32_
     size_t smem = smem_bytes(p);
     P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
-    long long grid = static_cast<long long>(T) * p.nblk * p.nsplit;
+    // T counts 1024-symbol plane tiles; the paired form runs 512-symbol tiles
+    long long grid = static_cast<long long>(p.paired ? plan_tiles(p, S) : T) * p.nblk * p.nsplit;
     if (grid > 0x7fffffffLL) {
         set_error("muladd grid too large");
         return P2G_ERANGE;
@@ -841,7 +1130,8 @@ int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdP
             return;
         for (const MuladdPlan &q : cands)
             if (q.warps == p.warps && q.ereg == p.ereg && q.nblk == p.nblk &&
-                q.nsplit == p.nsplit && q.psplit == p.psplit)
+                q.nsplit == p.nsplit && q.psplit == p.psplit && q.paired == p.paired &&
+                q.stage == p.stage)
                 return;
         cands.push_back(p);
     };
@@ -850,13 +1140,17 @@ int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdP
     for (const Variant &v0 : kVariants) {
         if (v0.small != small)
             continue;
-        // one pass per (warps, psplit) family: its largest compiled ereg
+        // one pass per (warps, psplit, form) family: its largest compiled ereg
         // sets the fewest output blocks; then the next two block counts, each
         // with the smallest compiled ereg that covers nout
+        auto same = [&](const Variant &v) {
+            return v.warps == v0.warps && v.psplit == v0.psplit && v.small == small &&
+                   v.paired == v0.paired && v.stage == v0.stage;
+        };
         bool first = true;
         int emax = 0;
         for (const Variant &v : kVariants) {
-            if (v.warps == v0.warps && v.psplit == v0.psplit && v.small == small) {
+            if (same(v)) {
                 emax = std::max(emax, v.ereg);
                 if (&v < &v0)
                     first = false;
@@ -864,14 +1158,14 @@ int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdP
         }
         if (!first)
             continue;
-        const int G = v0.warps / v0.psplit;
+        // outputs per block for each unit of ereg
+        const int G = v0.paired ? v0.warps * 2 : v0.warps / v0.psplit;
         const int nmin = (nout + G * emax - 1) / (G * emax);
         for (int nblk = nmin; nblk <= nmin + 2; ++nblk) {
             const int need = (nout + G * nblk - 1) / (G * nblk);
             int ereg = 0;
             for (const Variant &v : kVariants)
-                if (v.warps == v0.warps && v.psplit == v0.psplit && v.small == small &&
-                    v.ereg >= need && (ereg == 0 || v.ereg < ereg))
+                if (same(v) && v.ereg >= need && (ereg == 0 || v.ereg < ereg))
                     ereg = v.ereg;
             if (ereg == 0)
                 continue;
@@ -879,11 +1173,14 @@ int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdP
             p.warps = v0.warps;
             p.psplit = v0.psplit;
             p.small = small;
+            p.paired = v0.paired;
+            p.stage = v0.stage;
             p.ereg = ereg;
             p.nblk = nblk;
+            const int tiles = plan_tiles(p, S);
             for (int ns : {1, 2, 3, 4, 6, 8, 12, 16}) {
                 p.nsplit = ns;
-                const long long ctas = static_cast<long long>(T) * nblk * ns;
+                const long long ctas = static_cast<long long>(tiles) * nblk * ns;
                 if (ns > 1 && (nin / ns < 8 || ctas > 8LL * sms))
                     continue;
                 add(p);

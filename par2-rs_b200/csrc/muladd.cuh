@@ -69,6 +69,9 @@ int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchI
 // The plan for a problem: the context's tuned plan for this shape if there
 // is one, else a heuristic (8 warps, as many outputs per warp as fit).
 MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t slice_bytes);
+// Column tiles of plan p over slices of S bytes (1024 symbols each, 512 in
+// the paired form); a launch runs tiles x output blocks x input splits CTAs.
+int plan_tiles(const MuladdPlan &p, size_t S);
 // CTAs of plan p the device runs at once (SMs x CTAs resident per SM).
 int plan_slots(const p2g_ctx *ctx, const MuladdPlan &p);
 bool plan_valid(const MuladdPlan &p, int nin, int nout, size_t slice_bytes);

@@ -1,8 +1,11 @@
 // format_capi.cpp -- the C ABI of par2format.h over par2_pipeline.hpp.
 #include "../../include/par2format.h"
 
+#include <string.h>
+
 #include <string>
 
+#include "par2_codec.hpp"
 #include "par2_pipeline.hpp"
 
 namespace {
@@ -124,6 +127,29 @@ int p2f_repair_ex(const char *par2_path, const char *dir, int do_repair, int pur
         if (rebuilt)
             *rebuilt = n;
         fill(stats, r.stats());
+        return P2F_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+int p2f_streaming_encode(const uint8_t *const *src, size_t k, size_t block_size, size_t r,
+                         uint8_t *const *out, int threads)
+{
+    g_error.clear();
+    try {
+        if ((k && !src) || (r && !out))
+            throw par2::Par2Error("p2f_streaming_encode: null argument");
+        if (block_size % 2 != 0)
+            throw par2::Par2Error("Block size must be multiple of 2");
+        par2::Par2ReedSolomon codec(k, r);
+        par2::StreamingEncoder enc(codec.constants(), r, block_size,
+                                   threads > 0 ? static_cast<size_t>(threads) : 0);
+        for (size_t i = 0; i < k; ++i)
+            enc.process_block(i, reinterpret_cast<const uint16_t *>(src[i]), block_size / 2);
+        par2::RecoveryBlocks rec = enc.finalize();
+        for (size_t e = 0; e < r; ++e)
+            memcpy(out[e], rec[e].second.data(), rec[e].second.size());
         return P2F_OK;
     } catch (const std::exception &e) {
         return fail(e);

@@ -151,6 +151,29 @@ class CudaSm100aStrategy final : public GaloisSimdStrategy {
         check(p2g_muladd_region(ctx(), dsts, ndst, srcs, nsrc, coeffs, region_offset,
                                 region_size, 0));
     }
+    // shuffle2x: prepared buffers live on the device while the callers'
+    // loops record multiply-accumulates; finish runs them and copies back
+    bool supports_shuffle2x() const override { return p2g_supports_shuffle2x() != 0; }
+    void prepare_shuffle2x(uint16_t *data, size_t n) const override
+    {
+        check(p2g_prepare_shuffle2x(ctx(), data, n));
+    }
+    void finish_shuffle2x(uint16_t *data, size_t n) const override
+    {
+        check(p2g_finish_shuffle2x(ctx(), data, n));
+    }
+    void muladd_shuffle2x(uint16_t *dst, const uint16_t *src, size_t n,
+                          uint16_t scalar) const override
+    {
+        check(p2g_muladd_shuffle2x(ctx(), dst, src, n, scalar));
+    }
+    void muladd_region_shuffle2x(uint16_t *const *dsts, size_t ndst, const uint16_t *const *srcs,
+                                 size_t nsrc, const uint16_t *const *coeffs, size_t region_offset,
+                                 size_t region_size) const override
+    {
+        check(p2g_muladd_region_shuffle2x(ctx(), dsts, ndst, srcs, nsrc, coeffs, region_offset,
+                                          region_size));
+    }
     p2g_ctx *ctx() const
     {
         std::call_once(once_, [this] { check(p2g_create(device_, &ctx_)); });

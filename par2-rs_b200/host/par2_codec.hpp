@@ -5,7 +5,9 @@
 //   compute_reconstruction_transform         par2_rs.rs:319-422
 //   reconstruct_streaming_chunk              par2_rs.rs:442-675
 //   create_streaming_encoder                 par2_rs.rs:687-772
-//   StreamingEncoder::{process_block, finalize}  par2_rs.rs:775-902
+//   StreamingEncoder::{process_block, flush_batch, finalize}  par2_rs.rs:775-902
+//   galois dispatch (supports / prepare / finish_shuffle2x,
+//     gf_muladd_column[_shuffle2x])          galois/mod.rs:118-142, :248-349
 //
 // Same names, argument meaning and error strings.  The transform holds the
 // decode matrix A^-1 formed on the GPU (the reference records the elimination
@@ -16,9 +18,13 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
 #include <functional>
+#include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -47,44 +53,240 @@ inline p2g_ctx *codec_ctx()
     return strategy.ctx();
 }
 
+// Scalar GF(2^16) on the host (galois/core.rs:49-91, :175-193): the codec's
+// coefficient matrix needs c_i^e for every input i and exponent e.
+namespace gf {
+struct Tables {
+    uint16_t log[65536];
+    uint16_t exp[131070];
+    Tables()
+    {
+        uint32_t b = 1;
+        for (uint32_t l = 0; l < 65535; ++l) {
+            exp[l] = exp[l + 65535] = static_cast<uint16_t>(b);
+            log[b] = static_cast<uint16_t>(l);
+            b <<= 1;
+            if (b & 0x10000u)
+                b ^= 0x1100Bu;
+        }
+        log[0] = 0;
+    }
+};
+inline const Tables &tables()
+{
+    static const Tables *t = new Tables();
+    return *t;
+}
+inline uint16_t mul(uint16_t a, uint16_t b)
+{
+    if (!a || !b)
+        return 0;
+    const Tables &t = tables();
+    return t.exp[t.log[a] + t.log[b]];
+}
+}  // namespace gf
+
+// The galois/mod.rs entry points the codec calls, dispatched to the selected
+// strategy.  With no strategy selected they throw (the reference falls back
+// to its scalar code; this library has no CPU path).
+namespace galois {
+inline const GaloisSimdStrategy &selected()
+{
+    const GaloisSimdStrategy *s = get_registry().get_selected();
+    if (!s)
+        throw std::runtime_error("no galois strategy is available (no sm_100 device)");
+    return *s;
+}
+// galois/mod.rs:255-260
+inline bool supports_shuffle2x()
+{
+    const GaloisSimdStrategy *s = get_registry().get_selected();
+    return s && s->supports_shuffle2x();
+}
+// galois/mod.rs:274-282, :288-296
+inline void prepare_shuffle2x(uint16_t *data, size_t n)
+{
+    const GaloisSimdStrategy *s = get_registry().get_selected();
+    if (s && s->supports_shuffle2x())
+        s->prepare_shuffle2x(data, n);
+}
+inline void finish_shuffle2x(uint16_t *data, size_t n)
+{
+    const GaloisSimdStrategy *s = get_registry().get_selected();
+    if (s && s->supports_shuffle2x())
+        s->finish_shuffle2x(data, n);
+}
+// galois/mod.rs:118-142: dst[i] ^= source * coefficients[i], one strategy
+// call per non-zero coefficient
+inline void gf_muladd_column(uint16_t *const *dsts, size_t ndst, const uint16_t *src, size_t n,
+                             const uint16_t *coeffs)
+{
+    const GaloisSimdStrategy &s = selected();
+    for (size_t i = 0; i < ndst; ++i)
+        if (coeffs[i])
+            s.muladd(dsts[i], src, n, coeffs[i]);
+}
+// galois/mod.rs:328-349
+inline void gf_muladd_column_shuffle2x(uint16_t *const *dsts, size_t ndst, const uint16_t *src,
+                                       size_t n, const uint16_t *coeffs)
+{
+    const GaloisSimdStrategy &s = selected();
+    if (!s.supports_shuffle2x()) {
+        gf_muladd_column(dsts, ndst, src, n, coeffs);
+        return;
+    }
+    for (size_t i = 0; i < ndst; ++i)
+        if (coeffs[i])
+            s.muladd_shuffle2x(dsts[i], src, n, coeffs[i]);
+}
+}  // namespace galois
+
+// par2_rs.rs:88-126 (num_cpus: the host's thread count, or `threads`)
+inline size_t optimal_data_batch_size(size_t recovery_blocks, size_t num_cpus)
+{
+    const size_t base = recovery_blocks >= 100 ? num_cpus * 8
+                        : recovery_blocks >= 50 ? num_cpus * 4
+                                                : num_cpus * 2;
+    return std::min<size_t>(std::max<size_t>(base, 16), 128);
+}
+inline size_t optimal_recovery_batch_size(size_t recovery_blocks, size_t num_cpus)
+{
+    const size_t max_batch = std::max<size_t>(recovery_blocks / num_cpus, 1);
+    return std::min<size_t>(std::max<size_t>(max_batch, 4), 8);
+}
+
+// StreamingEncoder (par2_rs.rs:775-902), restated over the strategy
+// interface: data blocks are copied into reusable batch buffers (and
+// prepared when the strategy uses shuffle2x); a full batch is multiplied into
+// the recovery accumulators by worker threads, each taking recovery batches
+// of 4-8 blocks and calling the column multiply-accumulate once per buffered
+// data block (flush_batch, :816-870); finalize flushes the rest, finishes the
+// accumulators and returns them as little-endian bytes.  Worker threads take
+// recovery batches from a shared counter (the reference's rayon
+// par_chunks_mut).
 class StreamingEncoder {
   public:
-    StreamingEncoder(size_t data_blocks, size_t recovery_blocks, size_t block_size)
-        : k_(data_blocks), r_(recovery_blocks), bs_(block_size), data_(k_ * bs_, 0)
+    StreamingEncoder(const std::vector<uint16_t> &constants, size_t recovery_blocks,
+                     size_t block_size, size_t threads = 0)
+        : k_(constants.size()), r_(recovery_blocks), bs_(block_size), spb_(block_size / 2)
     {
+        threads_ = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+        // par2_rs.rs:707-719: coeff[i][e] = c_i^e by repeated multiplication
+        coeff_.assign(k_, std::vector<uint16_t>(r_));
+        for (size_t i = 0; i < k_; ++i) {
+            uint16_t c = 1;
+            for (size_t e = 0; e < r_; ++e) {
+                coeff_[i][e] = c;
+                c = gf::mul(c, constants[i]);
+            }
+        }
+        recovery_.assign(r_, std::vector<uint16_t>(spb_, 0));
+        use_shuffle2x_ = galois::supports_shuffle2x();
+        if (use_shuffle2x_)
+            for (auto &rb : recovery_)
+                galois::prepare_shuffle2x(rb.data(), rb.size());
+        data_batch_size_ = optimal_data_batch_size(r_, threads_);
+        recovery_batch_size_ = optimal_recovery_batch_size(r_, threads_);
+        batch_buffers_.assign(data_batch_size_, std::vector<uint16_t>(spb_, 0));
+        batch_indices_.reserve(data_batch_size_);
     }
-    // block_data_u16: the block as u16 symbols; indices beyond the data block
-    // count are ignored (par2_rs.rs:785-788).  Blocks never given count as zero.
+    size_t data_batch_size() const { return data_batch_size_; }
+    size_t recovery_batch_size() const { return recovery_batch_size_; }
+
+    // par2_rs.rs:785-807; indices beyond the data block count are ignored
     void process_block(size_t data_block_idx, const uint16_t *block_data_u16, size_t nsym)
     {
         if (data_block_idx >= k_)
             return;
-        const size_t n = std::min(nsym * 2, bs_);
-        memcpy(data_.data() + data_block_idx * bs_, block_data_u16, n);
+        const size_t slot = batch_indices_.size();
+        std::vector<uint16_t> &buffer = batch_buffers_[slot];
+        const size_t n = std::min(nsym, spb_);
+        memcpy(buffer.data(), block_data_u16, n * 2);
+        if (use_shuffle2x_)
+            galois::prepare_shuffle2x(buffer.data(), n);
+        batch_indices_.push_back(data_block_idx);
+        if (batch_indices_.size() >= data_batch_size_)
+            flush_batch();
     }
+
     // (exponent, bytes) for exponents 0..r-1 (par2_rs.rs:880-902)
     RecoveryBlocks finalize()
     {
+        flush_batch();
+        if (use_shuffle2x_)
+            for (auto &rb : recovery_)
+                galois::finish_shuffle2x(rb.data(), rb.size());
         RecoveryBlocks out(r_);
-        std::vector<const uint8_t *> src(k_);
-        std::vector<uint8_t *> dst(r_);
-        std::vector<uint32_t> exps(r_);
-        for (size_t i = 0; i < k_; ++i)
-            src[i] = data_.data() + i * bs_;
         for (size_t e = 0; e < r_; ++e) {
             out[e].first = static_cast<uint32_t>(e);
-            out[e].second.assign(bs_, 0);
-            dst[e] = out[e].second.data();
-            exps[e] = static_cast<uint32_t>(e);
+            out[e].second.resize(bs_ - bs_ % 2);
+            for (size_t x = 0; x < spb_; ++x) {
+                out[e].second[2 * x] = static_cast<uint8_t>(recovery_[e][x]);
+                out[e].second[2 * x + 1] = static_cast<uint8_t>(recovery_[e][x] >> 8);
+            }
         }
-        if (r_ && k_ && bs_)
-            check(p2g_encode(codec_ctx(), src.data(), k_, bs_, exps.data(), r_, dst.data(), 0));
         return out;
     }
 
   private:
-    size_t k_, r_, bs_;
-    std::vector<uint8_t> data_;
+    // par2_rs.rs:816-870
+    void flush_batch()
+    {
+        if (batch_indices_.empty())
+            return;
+        const size_t ntasks = (r_ + recovery_batch_size_ - 1) / recovery_batch_size_;
+        std::atomic<size_t> next{0};
+        std::exception_ptr err;
+        std::mutex err_mu;
+        auto worker = [&] {
+            std::vector<uint16_t *> dsts;
+            std::vector<uint16_t> coeffs;
+            for (size_t t; (t = next.fetch_add(1)) < ntasks;) {
+                const size_t b0 = t * recovery_batch_size_;
+                const size_t b1 = std::min(r_, b0 + recovery_batch_size_);
+                try {
+                    for (size_t slot = 0; slot < batch_indices_.size(); ++slot) {
+                        const uint16_t *data_block = batch_buffers_[slot].data();
+                        const std::vector<uint16_t> &c = coeff_[batch_indices_[slot]];
+                        dsts.clear();
+                        coeffs.clear();
+                        for (size_t e = b0; e < b1; ++e) {
+                            dsts.push_back(recovery_[e].data());
+                            coeffs.push_back(c[e]);
+                        }
+                        if (use_shuffle2x_)
+                            galois::gf_muladd_column_shuffle2x(dsts.data(), dsts.size(),
+                                                               data_block, spb_, coeffs.data());
+                        else
+                            galois::gf_muladd_column(dsts.data(), dsts.size(), data_block, spb_,
+                                                     coeffs.data());
+                    }
+                } catch (...) {
+                    std::lock_guard<std::mutex> lock(err_mu);
+                    if (!err)
+                        err = std::current_exception();
+                }
+            }
+        };
+        const size_t nthreads = std::min(threads_, ntasks);
+        std::vector<std::thread> pool;
+        for (size_t w = 1; w < nthreads; ++w)
+            pool.emplace_back(worker);
+        worker();
+        for (auto &th : pool)
+            th.join();
+        batch_indices_.clear();
+        if (err)
+            std::rethrow_exception(err);
+    }
+
+    size_t k_, r_, bs_, spb_, threads_;
+    std::vector<std::vector<uint16_t>> coeff_;
+    std::vector<std::vector<uint16_t>> recovery_;
+    bool use_shuffle2x_ = false;
+    std::vector<std::vector<uint16_t>> batch_buffers_;
+    std::vector<size_t> batch_indices_;
+    size_t data_batch_size_ = 16, recovery_batch_size_ = 4;
 };
 
 class Par2ReedSolomon {
@@ -109,7 +311,9 @@ class Par2ReedSolomon {
             if (b.size() != block_size)
                 throw Par2Error("Data block size mismatch: expected " + std::to_string(block_size) +
                                 ", got " + std::to_string(b.size()));
-        StreamingEncoder enc(data_blocks_, num_recovery, block_size);
+        // the streaming encoder's batched path (the reference's encode makes
+        // one strategy call per data x recovery block pair instead)
+        StreamingEncoder enc(constants_, num_recovery, block_size);
         for (size_t i = 0; i < data_blocks.size(); ++i)
             enc.process_block(i, reinterpret_cast<const uint16_t *>(data_blocks[i].data()),
                               block_size / 2);
@@ -125,7 +329,7 @@ class Par2ReedSolomon {
             throw Par2Error("Chunk size must be multiple of 2");
         if (chunk_size > block_size)
             throw Par2Error("Chunk size cannot exceed block size");
-        return StreamingEncoder(data_blocks_, recovery_blocks, block_size);
+        return StreamingEncoder(constants_, recovery_blocks, block_size);
     }
 
     // present_recovery_indices are block indices >= data_blocks (recovery

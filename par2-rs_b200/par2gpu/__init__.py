@@ -57,6 +57,11 @@ SIGNATURES = [
     ("p2g_hash_slices", _I, [_P, _P, _S, _S, _P, _P, _U32]),
     ("p2g_verify_slices", _I, [_P, _P, _S, _S, _P, _P, _P, _U32]),
     ("p2g_encode_noalloc", _I, [_P, _P, _S, _S, _P, _S, _P]),
+    ("p2g_supports_shuffle2x", _I, []),
+    ("p2g_prepare_shuffle2x", _I, [_P, _P, _S]),
+    ("p2g_muladd_shuffle2x", _I, [_P, _P, _P, _S, _U16]),
+    ("p2g_muladd_region_shuffle2x", _I, [_P, _P, _S, _P, _S, _P, _S, _S]),
+    ("p2g_finish_shuffle2x", _I, [_P, _P, _S]),
     ("p2g_batch_create", _I, [_P, _P, _S, _U32, _P]),
     ("p2g_batch_run", _I, [_P]),
     ("p2g_batch_launch", _I, [_P]),
@@ -90,7 +95,8 @@ class Plan(ctypes.Structure):
     """p2g_plan: tile shape of the multiply-accumulate kernel."""
     _fields_ = [("warps", ctypes.c_int), ("outputs_per_group", ctypes.c_int),
                 ("warps_per_group", ctypes.c_int), ("output_blocks", ctypes.c_int),
-                ("input_splits", ctypes.c_int), ("ms", ctypes.c_float)]
+                ("input_splits", ctypes.c_int), ("ms", ctypes.c_float),
+                ("tile_symbols", ctypes.c_int), ("inputs_per_stage", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -246,8 +252,9 @@ class Context:
         return p
 
     def set_plan(self, nin, nout, slice_bytes, warps, outputs_per_group, output_blocks,
-                 input_splits=1, warps_per_group=1):
-        p = Plan(warps, outputs_per_group, warps_per_group, output_blocks, input_splits, 0.0)
+                 input_splits=1, warps_per_group=1, tile_symbols=1024, inputs_per_stage=1):
+        p = Plan(warps, outputs_per_group, warps_per_group, output_blocks, input_splits, 0.0,
+                 tile_symbols, inputs_per_stage)
         check(lib().p2g_set_plan(self.h, nin, nout, slice_bytes, ctypes.byref(p)))
 
     # --- GaloisSimdStrategy mirror (galois/simd/mod.rs:36-58) -------------
@@ -268,6 +275,26 @@ class Context:
         check(lib().p2g_muladd_region(self.h, _ptr_array(dsts), len(dsts), _ptr_array(srcs),
                                       len(srcs), rows, region_offset, region_size,
                                       DEVICE_PTRS if device else 0))
+
+    # --- the shuffle2x hooks (galois/simd/mod.rs:68-127) ------------------
+    # Host u16 buffers (numpy uint16 arrays); between prepare and finish the
+    # context holds a device copy of each and records the multiply-accumulates.
+    def prepare_shuffle2x(self, buf):
+        check(lib().p2g_prepare_shuffle2x(self.h, buf.ctypes.data, buf.size))
+
+    def muladd_shuffle2x(self, dst, src, scalar):
+        check(lib().p2g_muladd_shuffle2x(self.h, dst.ctypes.data, src.ctypes.data,
+                                         min(dst.size, src.size), scalar))
+
+    def muladd_region_shuffle2x(self, dsts, srcs, coeffs, region_offset, region_size):
+        co = np.ascontiguousarray(coeffs, np.uint16).reshape(len(dsts), len(srcs))
+        rows = _ptr_array([co[d] for d in range(len(dsts))])
+        check(lib().p2g_muladd_region_shuffle2x(self.h, _ptr_array(dsts), len(dsts),
+                                                _ptr_array(srcs), len(srcs), rows,
+                                                region_offset, region_size))
+
+    def finish_shuffle2x(self, buf):
+        check(lib().p2g_finish_shuffle2x(self.h, buf.ctypes.data, buf.size))
 
     # --- coarse-grained encode (par2_rs.rs:687-902) -----------------------
     def encode(self, srcs, slice_bytes, exps, outs, device=False):

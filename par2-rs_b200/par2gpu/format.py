@@ -36,6 +36,8 @@ SIGNATURES = [
     ("p2f_repair_ex", [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, PROGRESS_FN,
                        ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
                        ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Stats)]),
+    ("p2f_streaming_encode", [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+                              ctypes.c_void_p, ctypes.c_int]),
     ("p2f_last_error", []),
 ]
 
@@ -109,3 +111,20 @@ def repair_ex(par2_path, directory, do_repair=True, purge=False, progress=None, 
                                ctypes.byref(cancel) if cancel is not None else None,
                                ctypes.byref(n), ctypes.byref(st)))
     return n.value, st
+
+
+def streaming_encode(src, r, threads=0):
+    """par2-rs's streaming encoder path over the strategy interface
+    (p2f_streaming_encode): src uint8 [k, S] host array -> recovery slices
+    uint8 [r, S] with exponents 0..r-1."""
+    import numpy as np
+
+    src = np.ascontiguousarray(src, np.uint8)
+    k, S = src.shape
+    out = np.zeros((r, S), np.uint8)
+    sp = (np.uint64(src.ctypes.data) + np.arange(k, dtype=np.uint64) * np.uint64(S)) if k \
+        else np.zeros(1, np.uint64)
+    op = (np.uint64(out.ctypes.data) + np.arange(r, dtype=np.uint64) * np.uint64(S)) if r \
+        else np.zeros(1, np.uint64)
+    _check(lib().p2f_streaming_encode(sp.ctypes.data, k, S, r, op.ctypes.data, threads))
+    return out

@@ -8,8 +8,10 @@
 #include <string.h>
 
 #include <map>
+#include <mutex>
 #include <random>
 #include <string>
+#include <thread>
 
 #include "../../par2-rs_b200/host/par2_codec.hpp"
 
@@ -95,7 +97,116 @@ static void test_registry()
     CudaSm100aStrategy cuda;
     CHECK(std::string(cuda.name()) == "CUDA-sm100a" && cuda.priority() == Priority::Optimal,
           "strategy identity");
-    CHECK(!cuda.supports_shuffle2x(), "no shuffle2x layout on the GPU strategy");
+    CHECK(cuda.supports_shuffle2x(), "the GPU strategy takes the shuffle2x hooks");
+}
+
+// A CPU strategy for the streaming encoder's call sequence: prepare_shuffle2x
+// changes the buffer in place (XOR with a mask) and finish_shuffle2x undoes
+// it, so a buffer used without a prepare or read without a finish gives wrong
+// results; the hooks also check that every multiply-accumulate names prepared
+// buffers and count the calls and the threads that made them.
+struct ShuffleFake final : GaloisSimdStrategy {
+    static constexpr uint16_t kMask = 0x5A5A;
+    mutable std::mutex mu;
+    mutable std::map<const uint16_t *, size_t> prepared;  // address -> symbols
+    mutable size_t calls = 0, violations = 0;
+    mutable std::map<std::thread::id, size_t> threads;
+    const char *name() const override { return "TestShuffle"; }
+    bool is_available() const override { return true; }
+    Priority priority() const override { return Priority::Optimal; }
+    void mul_slice(uint16_t c, uint16_t *d, size_t n) const override
+    {
+        for (size_t i = 0; i < n; ++i)
+            d[i] = gf_mul(d[i], c);
+    }
+    void muladd(uint16_t *dst, const uint16_t *src, size_t n, uint16_t c) const override
+    {
+        for (size_t i = 0; i < n; ++i)
+            dst[i] ^= gf_mul(src[i], c);
+    }
+    void muladd_region(uint16_t *const *, size_t, const uint16_t *const *, size_t,
+                       const uint16_t *const *, size_t, size_t) const override {}
+    bool supports_shuffle2x() const override { return true; }
+    void prepare_shuffle2x(uint16_t *d, size_t n) const override
+    {
+        for (size_t i = 0; i < n; ++i)
+            d[i] ^= kMask;
+        std::lock_guard<std::mutex> lock(mu);
+        prepared[d] = n;
+    }
+    void finish_shuffle2x(uint16_t *d, size_t n) const override
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!prepared.count(d))
+            ++violations;
+        prepared.erase(d);
+        for (size_t i = 0; i < n; ++i)
+            d[i] ^= kMask;
+    }
+    void muladd_shuffle2x(uint16_t *dst, const uint16_t *src, size_t n, uint16_t c) const override
+    {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            ++calls;
+            ++threads[std::this_thread::get_id()];
+            auto a = prepared.find(dst), b = prepared.find(src);
+            if (a == prepared.end() || b == prepared.end() || a->second < n || b->second < n)
+                ++violations;
+        }
+        for (size_t i = 0; i < n; ++i)
+            dst[i] = static_cast<uint16_t>(
+                ((dst[i] ^ kMask) ^ gf_mul(static_cast<uint16_t>(src[i] ^ kMask), c)) ^ kMask);
+    }
+};
+
+// StreamingEncoder (par2_rs.rs:775-902) over a strategy with shuffle2x: the
+// reference's batch sizes (par2_rs.rs:88-126), every data block prepared,
+// every accumulator prepared and finished, one call per (recovery block, data
+// block) pair from several worker threads, and the recovery slices of the
+// scalar definition.
+static void test_streaming_encoder()
+{
+    SimdRegistry &reg = get_registry();
+    auto owned = std::make_unique<ShuffleFake>();
+    const ShuffleFake *fake = owned.get();
+    reg.register_strategy(std::move(owned));
+    CHECK(reg.select_by_name("TestShuffle"), "select the test strategy");
+    CHECK(optimal_data_batch_size(205, 16) == 128 && optimal_data_batch_size(37, 4) == 16 &&
+              optimal_data_batch_size(60, 8) == 32,
+          "data batch sizes");
+    CHECK(optimal_recovery_batch_size(205, 16) == 8 && optimal_recovery_batch_size(37, 4) == 8 &&
+              optimal_recovery_batch_size(13, 8) == 4,
+          "recovery batch sizes");
+    const size_t k = 300, r = 37, bs = 96;
+    std::mt19937 rng(11);
+    std::vector<std::vector<uint8_t>> data(k, std::vector<uint8_t>(bs));
+    for (auto &b : data)
+        for (auto &x : b)
+            x = static_cast<uint8_t>(rng());
+    Par2ReedSolomon codec(k, r);
+    StreamingEncoder enc(codec.constants(), r, bs, 4);
+    CHECK(enc.data_batch_size() == 16 && enc.recovery_batch_size() == 8, "encoder batch sizes");
+    for (size_t i = 0; i < k; ++i)
+        enc.process_block(i, reinterpret_cast<const uint16_t *>(data[i].data()), bs / 2);
+    enc.process_block(k + 5, reinterpret_cast<const uint16_t *>(data[0].data()), bs / 2);
+    RecoveryBlocks rec = enc.finalize();
+    bool ok = rec.size() == r;
+    for (size_t e = 0; e < r && ok; ++e) {
+        ok = rec[e].first == e && rec[e].second.size() == bs;
+        for (size_t x = 0; x < bs / 2 && ok; ++x) {
+            uint16_t want = 0;
+            for (size_t i = 0; i < k; ++i) {
+                const uint16_t v = static_cast<uint16_t>(data[i][2 * x] | (data[i][2 * x + 1] << 8));
+                want ^= gf_mul(gf_pow(codec.constants()[i], static_cast<uint32_t>(e)), v);
+            }
+            ok = want == static_cast<uint16_t>(rec[e].second[2 * x] | (rec[e].second[2 * x + 1] << 8));
+        }
+    }
+    CHECK(ok, "recovery slices equal sum_i c_i^e D_i");
+    CHECK(fake->calls == k * r, "one call per (recovery, data) pair: %zu", fake->calls);
+    CHECK(fake->violations == 0, "every call on prepared buffers, every finish after a prepare");
+    CHECK(fake->threads.size() > 1, "the batches ran on several threads (%zu)", fake->threads.size());
+    reg.select_best();
 }
 
 static void test_each_simd_strategy()
@@ -265,6 +376,7 @@ int main(int argc, char **argv)
     try {
         if (what == "registry") {
             test_registry();
+            test_streaming_encoder();
         } else {
             test_each_simd_strategy();
             test_codec();

@@ -195,6 +195,70 @@ def test_every_tile_shape_matches_oracle(ctx):
             assert np.array_equal(got, want), (W, E, P, nblk, ns)
 
 
+PAIRED = [(8, e, 1) for e in range(7, 14)] + [(12, 8, 1)] + \
+    [(8, e, 2) for e in (7, 9, 11, 13)] + [(12, 8, 2)]
+
+
+@pytest.mark.parametrize("r", [25, 105, 151, 205, 209])
+def test_every_paired_shape_matches_oracle(ctx, r):
+    """The paired form (512-symbol tiles, half a warp per output): every
+    compiled shape, one or two inputs per barrier, that covers r in at most
+    three output blocks, with and without input splits (odd and even input
+    counts per split), on a ragged last tile (an odd number of 512-symbol
+    tiles, the last one partial) and an odd output count (the last pair of a
+    block half empty), gives the oracle's recovery slices."""
+    rng = np.random.default_rng(500 + r)
+    k, S = 41, 1024 * 4 + 68
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = rng.choice(3000, r, replace=False).astype(np.uint32)
+    want = oracle.encode(src, exps)
+    ran = 0
+    for W, E, G in PAIRED:
+        per = W * E * 2
+        for nblk in (-(-r // per), -(-r // per) + 1):
+            if (nblk - 1) * per >= r or nblk > 3:
+                continue
+            for ns in (1, 3):
+                ctx.set_plan(k, r, S, W, 2 * E, nblk, ns, 1, tile_symbols=512,
+                             inputs_per_stage=G)
+                assert np.array_equal(ctx.encode_array(src, exps), want), (W, E, G, nblk, ns)
+                ran += 1
+    assert ran > 0
+
+
+def test_paired_form_in_accumulating_groups_and_repair(ctx):
+    """The heuristic picks the paired form above 104 outputs: 300 host inputs
+    go up in groups whose later passes accumulate into the outputs; a 150-slice
+    repair runs both of its passes (store, then accumulate) on it."""
+    rng = np.random.default_rng(77)
+    k, S, r = 300, 4096 + 1024, 205
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(r, dtype=np.uint32)
+    rec = ctx.encode_array(src, exps)
+    assert np.array_equal(rec, oracle.encode(src, exps))
+    m = 150
+    missing = np.sort(rng.choice(k, m, replace=False))
+    data = src.copy()
+    data[missing] = 0
+    got = ctx.repair_array(data, missing, exps[:m], rec[:m])
+    assert np.array_equal(got, src[missing])
+
+
+def test_set_plan_rejects_bad_paired_shapes(ctx):
+    import par2gpu
+
+    for bad in [dict(outputs_per_group=13, tile_symbols=512),   # odd: not whole pairs
+                dict(outputs_per_group=26, tile_symbols=256),   # no such tile
+                dict(outputs_per_group=30, tile_symbols=512),   # not compiled
+                dict(outputs_per_group=20, tile_symbols=512, inputs_per_stage=2),  # not compiled
+                dict(outputs_per_group=13, tile_symbols=1024, inputs_per_stage=2)]:
+        with pytest.raises(par2gpu.Par2GpuError) as ei:
+            ctx.set_plan(40, 150 if bad["tile_symbols"] != 1024 else 100, 4096, 8,
+                         bad["outputs_per_group"], 1, 1, 1, tile_symbols=bad["tile_symbols"],
+                         inputs_per_stage=bad.get("inputs_per_stage", 1))
+        assert ei.value.code == par2gpu.EINVAL
+
+
 @pytest.mark.parametrize("r", [1, 5, 8, 9, 16, 17, 24, 25])
 def test_small_output_tables_match_oracle(ctx, r):
     """Up to 24 outputs the kernel uses the 6 + 5 + 5 tables (24-word
