@@ -562,16 +562,21 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
                 planes + (static_cast<size_t>(i) * T + t) * 512 + hsel * 16);
             const uint8_t *gr = reinterpret_cast<const uint8_t *>(
                 recs + (static_cast<size_t>(i) * nout + obase) * kRecordWords);
-            const int nchunk = 64 + nb * (kRecordWords / 4);
+            // an odd block's last record is copied twice, so that the
+            // second output of its last pair reads valid offsets
+            const int nchunk = 64 + (nb + (nb & 1)) * (kRecordWords / 4);
             for (int c = threadIdx.x; c < nchunk; c += THREADS) {
                 // plane b goes to position 2 (b % 8) + b / 8, so that planes
                 // b and b + 8, read together by the two halves of a warp in
                 // the build, share one 128-byte row of banks
-                if (c < 64)
+                if (c < 64) {
                     cp_async16(s + (((c >> 2) & 7) * 2 + (c >> 5)) * 64 + (c & 3) * 16,
                                gp + (c >> 2) * 128 + (c & 3) * 16);
-                else
-                    cp_async16(s + kPairTileBytes + (c - 64) * 16, gr + (c - 64) * 16);
+                } else {
+                    const int rc = c - 64;
+                    cp_async16(s + kPairTileBytes + rc * 16,
+                               gr + (rc < nb * (kRecordWords / 4) ? rc : rc - 4) * 16);
+                }
             }
         }
         cp_async_commit();
@@ -624,27 +629,30 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
 
     // As an address giver, lane L serves matrix m = L / 8 for output s =
     // (L / 4) & 1 of the pair (chunk L % 4 of that output's half-row) and
-    // reads record class m ^ s of output s; the last output of an odd block
-    // reads the block's last record instead (its sums are never stored).
+    // reads record class m ^ s of output s.  A lane's class fixes which table
+    // it reads: even classes hold T0 offsets n * 128, odd classes T1 offsets
+    // (n + 256) * 128, and the T1 half-row of combined row n sits at
+    // n * 128 + 64, so T1 readers take the base tab + 64 - 32768 (32-bit
+    // shared addresses wrap) and both use the record offsets unchanged.  The
+    // second output of an odd block's last pair reads the duplicated last
+    // record (its sums are never stored).
     const int gs = (lane >> 2) & 1;
     const int gcls = (lane >> 3) ^ gs;
-    const uint32_t tab_s = static_cast<uint32_t>(__cvta_generic_to_shared(tab)) + (lane & 3) * 16;
+    const uint32_t tab_s = static_cast<uint32_t>(__cvta_generic_to_shared(tab)) + (lane & 3) * 16 +
+                           ((gcls & 1) ? 64u - 32768u : 0u);
     auto consume = [&](int i, int buf) {
-        const uint4 *R = reinterpret_cast<const uint4 *>(slot(i) + kPairTileBytes);
+        const uint4 *R = reinterpret_cast<const uint4 *>(slot(i) + kPairTileBytes) +
+                         (2 * q0 + gs) * 4 + gcls;
         const uint32_t tb = tab_s + buf * TW * 4;
         // the next pair's record is loaded before this pair's lookups
-        uint4 nxt = R[min(2 * q0 + gs, nb - 1) * 4 + gcls];
+        uint4 nxt = myq > 0 ? R[0] : make_uint4(0, 0, 0, 0);
 #pragma unroll
         for (int e = 0; e < EREG; ++e) {
             if (e < myq) {
                 const uint4 r = nxt;
-                if (e + 1 < EREG)
-                    nxt = R[min(2 * (q0 + e + 1) + gs, nb - 1) * 4 + gcls];
-                // (n + 256 t) * 128 -> n * 128 + 64 t, both halves of a word
-                uint32_t w[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    w[q] = (w[q] & 0x7FFF7FFFu) | ((w[q] >> 9) & 0x00400040u);
+                if (e + 1 < myq)
+                    nxt = R[(e + 1) * 8];
+                const uint32_t w[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
                 for (int p = 0; p < 8; ++p) {
                     const uint32_t off = (p & 1) ? (w[p >> 1] >> 16) : (w[p >> 1] & 0xFFFFu);
