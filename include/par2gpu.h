@@ -297,7 +297,7 @@ int p2g_batch_destroy(p2g_batch *batch);
  *     P2G_NOALLOC_SCRATCH_BYTES on every GPU that loads this library, held
  *     until the process exits.  A problem's scratch is about k*r*98 bytes
  *     when r <= 24 (2-byte coefficient + 96-byte record per pair) or
- *     k*r*66 bytes when r > 24 (64-byte records), plus k*slice_bytes rounded
+ *     k*r*34 bytes when r > 24 (32-byte records), plus k*slice_bytes rounded
  *     up to 2 KiB tiles, plus the pointer tables; a problem that needs more
  *     than the array returns P2G_ERANGE.
  *   - src[k] / out[r] are 16-byte aligned DEVICE pointers on the current

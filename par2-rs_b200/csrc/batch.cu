@@ -478,7 +478,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
         for (const Prob &p : probs)
             if (p.phase == x) {
                 pl += static_cast<size_t>(p.nin) * ((p.S + 2047) / 2048) * 2048;
-                rc += static_cast<size_t>(p.nin) * p.nout * 64;
+                rc += static_cast<size_t>(p.nin) * p.nout * kRecordWords * 4;
             }
         plane_need = std::max(plane_need, pl);
         rec_need = std::max(rec_need, rc);
@@ -572,7 +572,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
                 }
             }
             pl_off += static_cast<size_t>(p.nin) * T * 2048;
-            rc_off += static_cast<size_t>(p.nin) * p.nout * 64;
+            rc_off += static_cast<size_t>(p.nin) * p.nout * kRecordWords * 4;
             pl_first += static_cast<unsigned long long>(p.nin) * T * 32;
             rc_first += static_cast<unsigned long long>(p.nin) * p.nout;
         }

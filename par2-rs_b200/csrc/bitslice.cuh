@@ -63,27 +63,28 @@ __host__ __device__ __forceinline__ uint32_t gf_times_x(uint32_t v)
 // Row stride of a lookup table in shared memory: one 32-bit word per lane.
 constexpr uint32_t kRowBytes = 128;
 
-// The 16-word "record" of a coefficient c.  The 16 input planes are split in
+// The 8-word "record" of a coefficient c.  The 16 input planes are split in
 // two halves of 8; for each half a 256-row table holds every XOR combination
-// of its planes (row n = XOR of the planes whose bit is set in n; T1 follows
-// T0, rows of 128 bytes: one word per lane).  Output plane j is then
+// of its planes (row n = XOR of the planes whose bit is set in n; rows of 128
+// bytes: one word per lane).  Output plane j is then
 //   T0[n0_j] ^ T1[n1_j],  n0_j = sum_{b<8} bit_j(c x^b) << b,
 //                         n1_j = sum_{b<8} bit_j(c x^{b+8}) << b.
 // The rows are fetched four at a time with ldmatrix.x4 (matrix m's eight
-// 16-byte row pointers come from lanes 8m..8m+7, so lane L receives word L of
-// each of the four rows).  For plane pair p (planes 2p, 2p+1) the four rows are
-//   m = 0: T0[n0_2p]   m = 1: T1[n1_2p]   m = 2: T0[n0_2p+1]   m = 3: T1[n1_2p+1]
-// and word 4m + i of the record holds the byte offsets of matrix m's rows for
-// p = 2i (low half) and p = 2i+1 (high half), so lane L reads the 16 bytes at
-// word 4*(L/8) and needs no other record data.
-__host__ __device__ __forceinline__ uint32_t row_offset(int m, uint32_t n0[16], uint32_t n1[16],
-                                                        int p)
+// 16-byte row pointers come from lanes 8m..8m+7).  For plane pair p (planes
+// 2p, 2p+1) the four rows are
+//   class 0: T0[n0_2p]   class 1: T1[n1_2p]   class 2: T0[n0_2p+1]   class 3: T1[n1_2p+1]
+// and byte p of record words 2m, 2m + 1 (little-endian, 8 bytes) holds the
+// row index of class m for plane pair p, so a lane reads the 8 bytes of its
+// class and needs no other record data.  Odd classes index T1, even T0: the
+// reader folds the table into its lane's base address.
+__host__ __device__ __forceinline__ uint32_t row_index(int m, const uint32_t n0[16],
+                                                       const uint32_t n1[16], int p)
 {
     const int j = 2 * p + (m >> 1);
-    return (m & 1) ? (256u + n1[j]) * kRowBytes : n0[j] * kRowBytes;
+    return (m & 1) ? n1[j] : n0[j];
 }
 
-__host__ __device__ __forceinline__ void make_record(uint32_t c, uint32_t w[16])
+__host__ __device__ __forceinline__ void make_record(uint32_t c, uint32_t w[8])
 {
     uint32_t col[16];
     uint32_t v = c & 0xFFFFu;
@@ -107,12 +108,17 @@ __host__ __device__ __forceinline__ void make_record(uint32_t c, uint32_t w[16])
 #pragma unroll
     for (int m = 0; m < 4; ++m)
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-            w[4 * m + i] = row_offset(m, n0, n1, 2 * i) | (row_offset(m, n0, n1, 2 * i + 1) << 16);
+        for (int h = 0; h < 2; ++h) {
+            uint32_t x = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                x |= row_index(m, n0, n1, 4 * h + q) << (8 * q);
+            w[2 * m + h] = x;
+        }
 }
 
 // Words per record of the two table forms.
-constexpr int kRecordWords = 16;
+constexpr int kRecordWords = 8;
 constexpr int kRecordWordsSmall = 24;
 
 // The small-output form (6 + 5 + 5 planes): three tables of 64, 32 and 32
@@ -161,7 +167,7 @@ __host__ __device__ __forceinline__ void make_record_small(uint32_t c, uint32_t 
 
 #ifdef __CUDACC__
 // Writes record idx of coefficient c in the small (24-word) or the 8 + 8
-// (16-word) form; records are 16-byte aligned in both.
+// (8-word) form; records are 16-byte aligned in both.
 __device__ __forceinline__ void write_record(uint32_t *recs, size_t idx, uint32_t c, bool small)
 {
     if (small) {

@@ -17,10 +17,11 @@
 //   * Per input slice the CTA builds, in shared memory, two 256-row tables of
 //     every XOR combination of planes 0-7 and of planes 8-15 (64 KiB, lane L's
 //     column in bank L).  One output plane of one coefficient is then two
-//     table rows XORed; the rows to read are the coefficient's "record" (16
-//     words), the same for all 32 lanes.  ldmatrix.x4 serves as a 4-row
-//     gather: one instruction hands every lane its own word of four rows, so
-//     a coefficient costs 8 ldmatrix + 1 record load + 16 XORs per lane.
+//     table rows XORed; the rows to read are the coefficient's "record" (32
+//     row-index bytes), the same for all 32 lanes.  ldmatrix.x4 serves as a
+//     4-row gather: one instruction hands every lane its own word of four
+//     rows, so a coefficient costs 8 ldmatrix + 1 record load + 16 XORs per
+//     lane.
 //   * The next input's planes and records stream into a 4-slot shared-memory
 //     ring with cp.async while the current table is consumed; the table is
 //     double-buffered, one CTA barrier per input slice.
@@ -345,8 +346,11 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
 
     // Lane L fetches, per plane pair, word L of four table rows with one
     // ldmatrix.x4; it supplies the address of 16-byte chunk (L % 8) of the
-    // row of matrix L / 8 (record layout: bitslice.cuh make_record).
-    const uint32_t tab_s = static_cast<uint32_t>(__cvta_generic_to_shared(tab)) + (lane & 7) * 16;
+    // row of class L / 8, read from its class's 8 record bytes (bitslice.cuh
+    // make_record).  Odd classes read T1, whose rows follow T0's 256: their
+    // lanes' base address carries the 32 KiB.
+    const uint32_t tab_s = static_cast<uint32_t>(__cvta_generic_to_shared(tab)) + (lane & 7) * 16 +
+                           ((!SMALL && ((lane >> 3) & 1)) ? 256u * 128u : 0u);
     auto consume_small = [&](int i, int buf) {
         // lane group m's six record words: 3 x 8 bytes at word 6m of each record
         const uint2 *R = reinterpret_cast<const uint2 *>(ring + (i & (kRing - 1)) * SLOT +
@@ -382,37 +386,37 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
             consume_small(i, buf);
             return;
         }
-        const uint4 *R = reinterpret_cast<const uint4 *>(ring + (i & (kRing - 1)) * SLOT +
+        // lane group m's 8 record bytes: words 2m, 2m + 1
+        const uint2 *R = reinterpret_cast<const uint2 *>(ring + (i & (kRing - 1)) * SLOT +
                                                          kTileBytes) +
                          my0 * 4 + (lane >> 3);
         const uint32_t tb = tab_s + buf * kTableBytes;
         // the next output's record is loaded before this output's lookups, so
-        // it does not wait behind them in the shared-memory queue (loads past
-        // the block's last output stay inside the ring slot and go unused)
-        uint4 nxt = R[0];
+        // it does not wait behind them in the shared-memory queue
+        uint2 nxt = make_uint2(0, 0);
+        if constexpr (PSPLIT == 1)
+            if (myn > 0)
+                nxt = R[0];
 #pragma unroll
         for (int e = 0; e < EREG; ++e) {
             if (e < myn) {
-                uint32_t w[4];
+                uint32_t w[2];
                 if constexpr (PSPLIT == 1) {
-                    const uint4 r = nxt;
-                    if (e + 1 < EREG)
+                    const uint2 r = nxt;
+                    if (e + 1 < myn)
                         nxt = R[(e + 1) * 4];
                     w[0] = r.x;
                     w[1] = r.y;
-                    w[2] = r.z;
-                    w[3] = r.w;
                 } else {
-                    // plane pairs [4ph, 4ph+4): record words 2ph, 2ph+1
-                    const uint2 r = reinterpret_cast<const uint2 *>(R + e * 4)[ph];
-                    w[0] = r.x;
-                    w[1] = r.y;
+                    // plane pairs [4ph, 4ph+4): record word 2m + ph
+                    w[0] = reinterpret_cast<const uint32_t *>(R + e * 4)[ph];
+                    w[1] = 0;
                 }
 #pragma unroll
                 for (int p = 0; p < NPL / 2; ++p) {
-                    const uint32_t off = (p & 1) ? (w[p >> 1] >> 16) : (w[p >> 1] & 0xFFFFu);
+                    const uint32_t row = __byte_perm(w[p >> 2], 0u, 0x4440u | (p & 3));
                     uint32_t d0, d1, d2, d3;
-                    ldsm_x4(tb + off, d0, d1, d2, d3);
+                    ldsm_x4(tb + (row << 7), d0, d1, d2, d3);
                     acc[e][2 * p] ^= d0 ^ d1;
                     acc[e][2 * p + 1] ^= d2 ^ d3;
                 }
@@ -516,11 +520,10 @@ __global__ void __launch_bounds__(WARPS * 32, SMALL ? 2 : 1)
 //   matrix 0: lanes 0-15 T0[n0_2k(A)], lanes 16-31 T1[n1_2k(B)]
 //   matrix 1: lanes 0-15 T1[n1_2k(A)], lanes 16-31 T0[n0_2k(B)]
 //   matrix 2, 3: the same for plane 2k + 1
-// (A, B: the outputs of the two halves).  Records are the 16-word records of
-// the 1024-symbol form (bitslice.cuh make_record): record word 4m + i holds the
-// class-m offsets, and the lanes that give matrix m's addresses for output B
-// read class m ^ 1, whose T0 / T1 roles are swapped.  A record offset
-// (n + 256 t) * 128 becomes n * 128 + 64 t here.
+// (A, B: the outputs of the two halves).  Records are the 8-word records of
+// the 1024-symbol form (bitslice.cuh make_record): record words 2m, 2m + 1
+// hold the class-m row indices, and the lanes that give matrix m's addresses
+// for output B read class m ^ 1, whose T0 / T1 roles are swapped.
 template <int WARPS, int EREG, int STAGE>
 __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t *__restrict__ planes,
                                                    const uint32_t *__restrict__ recs, int nout,
@@ -575,7 +578,7 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
                 } else {
                     const int rc = c - 64;
                     cp_async16(s + kPairTileBytes + rc * 16,
-                               gr + (rc < nb * (kRecordWords / 4) ? rc : rc - 4) * 16);
+                               gr + (rc < nb * (kRecordWords / 4) ? rc : rc - kRecordWords / 4) * 16);
                 }
             }
         }
@@ -629,35 +632,32 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
 
     // As an address giver, lane L serves matrix m = L / 8 for output s =
     // (L / 4) & 1 of the pair (chunk L % 4 of that output's half-row) and
-    // reads record class m ^ s of output s.  A lane's class fixes which table
-    // it reads: even classes hold T0 offsets n * 128, odd classes T1 offsets
-    // (n + 256) * 128, and the T1 half-row of combined row n sits at
-    // n * 128 + 64, so T1 readers take the base tab + 64 - 32768 (32-bit
-    // shared addresses wrap) and both use the record offsets unchanged.  The
-    // second output of an odd block's last pair reads the duplicated last
-    // record (its sums are never stored).
+    // reads the 8 record bytes of class m ^ s of output s.  Odd classes index
+    // T1, whose half-row of combined row n sits at n * 128 + 64: their lanes'
+    // base address carries the 64.  The second output of an odd block's last
+    // pair reads the duplicated last record (its sums are never stored).
     const int gs = (lane >> 2) & 1;
     const int gcls = (lane >> 3) ^ gs;
     const uint32_t tab_s = static_cast<uint32_t>(__cvta_generic_to_shared(tab)) + (lane & 3) * 16 +
-                           ((gcls & 1) ? 64u - 32768u : 0u);
+                           (gcls & 1) * 64;
     auto consume = [&](int i, int buf) {
-        const uint4 *R = reinterpret_cast<const uint4 *>(slot(i) + kPairTileBytes) +
+        const uint2 *R = reinterpret_cast<const uint2 *>(slot(i) + kPairTileBytes) +
                          (2 * q0 + gs) * 4 + gcls;
         const uint32_t tb = tab_s + buf * TW * 4;
         // the next pair's record is loaded before this pair's lookups
-        uint4 nxt = myq > 0 ? R[0] : make_uint4(0, 0, 0, 0);
+        uint2 nxt = myq > 0 ? R[0] : make_uint2(0, 0);
 #pragma unroll
         for (int e = 0; e < EREG; ++e) {
             if (e < myq) {
-                const uint4 r = nxt;
+                const uint2 r = nxt;
                 if (e + 1 < myq)
                     nxt = R[(e + 1) * 8];
-                const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+                const uint32_t w[2] = {r.x, r.y};
 #pragma unroll
                 for (int p = 0; p < 8; ++p) {
-                    const uint32_t off = (p & 1) ? (w[p >> 1] >> 16) : (w[p >> 1] & 0xFFFFu);
+                    const uint32_t row = __byte_perm(w[p >> 2], 0u, 0x4440u | (p & 3));
                     uint32_t d0, d1, d2, d3;
-                    ldsm_x4(tb + off, d0, d1, d2, d3);
+                    ldsm_x4(tb + (row << 7), d0, d1, d2, d3);
                     acc[e][2 * p] ^= d0 ^ d1;
                     acc[e][2 * p + 1] ^= d2 ^ d3;
                 }

@@ -8,7 +8,7 @@ namespace p2g {
 // Problems of at most this many outputs use the small-output tables (6 + 5 +
 // 5 planes: 128 table rows per input instead of 512, 48 row reads per
 // coefficient instead of 32; cheaper below ~24 outputs) and 24-word records;
-// larger ones the 8 + 8 tables and 16-word records.  The form follows from
+// larger ones the 8 + 8 tables and 8-word records.  The form follows from
 // the output count alone, so records built for a problem always match the
 // kernel that reads them.
 constexpr int kSmallOutputs = 24;
@@ -22,7 +22,7 @@ inline size_t record_bytes(size_t nin, int nout)
 // One multiply-accumulate problem of a batch (device-resident description).
 struct BatchProb {
     const uint32_t *planes;  // [nin][T][512]
-    const uint32_t *recs;    // [nin][nout][16] (the batch kernel uses the 8 + 8 tables)
+    const uint32_t *recs;    // [nin][nout][8] (the batch kernel uses the 8 + 8 tables)
     uint8_t *const *dst;     // nout device pointers
     size_t S;                // bytes per slice
     int nin, nout, T, nblk, nsplit, mode;

@@ -59,10 +59,15 @@ class ServedJob:
         return self.k * self.n * cols // 2
 
     def scratch_bytes(self):
-        """What admission reserves: outputs, bit planes, coefficient records."""
+        """What admission reserves: outputs, bit planes (whole 2 KiB tiles),
+        coefficient records (96 bytes per pair up to 24 outputs, else 32)
+        and, for a repair, the right-hand sides of its first pass."""
         if self.kind == "verify":
             return self.k * 20
-        return self.n * self.S + self.k * self.S + self.k * self.n * 64 + self.n * self.S
+        planes = self.k * (-(-self.S // 2048) * 2048)
+        records = self.k * self.n * (96 if self.n <= 24 else 32)
+        rhs = self.n * self.S if self.kind == "repair" else 0
+        return self.n * self.S + planes + records + rhs
 
 
 def _alloc_outputs(job):

@@ -60,9 +60,9 @@ static void apply_wide(const uint32_t planes[16], uint32_t c, uint32_t out[16])
     for (int p = 0; p < 8; ++p) {
         uint32_t d[4];
         for (int m = 0; m < 4; ++m) {
-            const uint32_t word = w[4 * m + (p >> 1)];
-            const uint32_t off = (p & 1) ? (word >> 16) : (word & 0xFFFFu);
-            d[m] = tab[off / kRowBytes];
+            // byte p of class m's two record words; odd classes index T1
+            const uint32_t row = (w[2 * m + (p >> 2)] >> (8 * (p & 3))) & 0xFFu;
+            d[m] = tab[row + ((m & 1) ? 256u : 0u)];
         }
         out[2 * p] ^= d[0] ^ d[1];
         out[2 * p + 1] ^= d[2] ^ d[3];
