@@ -53,7 +53,7 @@ constexpr int kRing = 4;
 constexpr int kPairTileBytes = 1024;          // 512 symbols (paired form)
 constexpr int kPairTableWords = 256 * 32;     // 256 combined rows of 128 B
 // ring slots of the paired form with one / two inputs per CTA barrier
-__host__ __device__ constexpr int pair_ring_slots(int stage) { return stage == 1 ? 4 : 6; }
+__host__ __device__ constexpr int pair_ring_slots(int stage) { return stage == 1 ? 4 : 8; }
 
 // Four 8x8 b16 matrices from shared memory: lanes 8m..8m+7 give the row
 // addresses of matrix m, lane L receives word L % 4 of row L / 4 of each.
@@ -685,26 +685,26 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
             }
         }
     } else {
-        // two inputs per barrier (four table buffers, six ring slots): stage
-        // s consumes inputs s, s + 1 from one table pair, builds s + 2, s + 3
-        // into the other, and fetches s + 4, s + 5, which land before the
-        // barrier that ends the stage
+        // two inputs per barrier (four table buffers, eight ring slots):
+        // stage s consumes inputs s, s + 1 from one table pair, builds s + 2,
+        // s + 3 into the other and fetches s + 6, s + 7, whose copies may
+        // still be in flight at the barrier that ends the stage (s + 4, s + 5,
+        // fetched a stage earlier, must have landed by then)
         if (i0 < i1) {
-            issue(i0);
-            issue(i0 + 1);
-            issue(i0 + 2);
-            issue(i0 + 3);
-            cp_async_wait<2>();
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                issue(i0 + q);
+            cp_async_wait<4>();
             __syncthreads();
             build(i0, 0);
             if (i0 + 1 < i1)
                 build(i0 + 1, 1);
-            cp_async_wait<0>();
+            cp_async_wait<2>();
             __syncthreads();
             for (int s = i0; s < i1; s += 2) {
                 const int tp = ((s - i0) >> 1) & 1;
-                issue(s + 4);
-                issue(s + 5);
+                issue(s + 6);
+                issue(s + 7);
                 if (s + 2 < i1)
                     build(s + 2, 2 * (tp ^ 1));
                 if (s + 3 < i1)
@@ -712,7 +712,7 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
                 consume(s, 2 * tp);
                 if (s + 1 < i1)
                     consume(s + 1, 2 * tp + 1);
-                cp_async_wait<0>();
+                cp_async_wait<2>();
                 __syncthreads();
             }
         }
