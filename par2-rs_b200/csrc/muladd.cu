@@ -939,7 +939,9 @@ MuladdPlan choose_plan(const p2g_ctx *ctx, int nin, int nout, size_t S)
         p.paired = true;
         p.nblk = (nout + 8 * 13 * 2 - 1) / (8 * 13 * 2);
         const int pairs = ((nout + p.nblk - 1) / p.nblk + 1) / 2;
-        p.ereg = std::max(7, (pairs + 7) / 8);
+        // two inputs per barrier (compiled for odd pair counts 7-13 per warp)
+        p.ereg = std::max(7, (pairs + 7) / 8) | 1;
+        p.stage = 2;
     } else {
         p.nblk = (nout + 8 * 13 - 1) / (8 * 13);
         p.ereg = std::max(1, (nout + 8 * p.nblk - 1) / (8 * p.nblk));
