@@ -909,9 +909,17 @@ def batched_leg():
             b.close()
             assert all(v == 0 for v in stv), stv
 
+    # the batch kernel's tile form per problem class, tuned on this device
+    # before anything is timed
+    forms, form_ms = ctx.batch_autotune(reps=2)
+    names = {par2gpu.FORM_WIDE: "wide", par2gpu.FORM_SMALL: "small",
+             par2gpu.FORM_PAIRED: "paired"}
     out = {"workload": "batched: 256 sets, file sizes log-uniform 64 KiB-256 MiB, slices "
                        "{4,16,64,256,1024} KiB, redundancy 1-20%, half create / half repair",
-           "sets": len(sets), "source_bytes": total_src, "batches": len(groups)}
+           "sets": len(sets), "source_bytes": total_src, "batches": len(groups),
+           "tuned_forms": {f"outputs {o}, slices {sz}": names[forms[2 * i + j]]
+                           for i, o in enumerate(("1-24", "25-104", "105-208", ">208"))
+                           for j, sz in enumerate(("<=16KiB", ">16KiB"))}}
     for name, fn in (("plain", plain_all), ("batched", batched_all)):
         fn()  # warm-up
         torch.cuda.synchronize(dev)

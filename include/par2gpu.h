@@ -285,6 +285,32 @@ int p2g_batch_wait(p2g_batch *batch);
 int p2g_batch_cancel(p2g_batch *batch);
 int p2g_batch_destroy(p2g_batch *batch);
 
+/* Tile forms of the persistent batch kernel; each problem of a batch runs in
+ * the form chosen for its class.  No counterpart in par2-rs, which runs one
+ * recovery set per process (par2_rs.rs:816-870) with the blocking its
+ * strategy fixes (avx2.rs:700-701). */
+#define P2G_FORM_WIDE 0   /* 8 + 8 tables over 1024-symbol tiles, 104 outputs per item */
+#define P2G_FORM_SMALL 1  /* 6 + 5 + 5 tables, at most 24 outputs */
+#define P2G_FORM_PAIRED 2 /* 8 + 8 tables over 512-symbol tiles, 208 outputs per item */
+/* Problem classes: 2 * (outputs 1-24: 0, 25-104: 1, 105-208: 2, more: 3)
+ * + (slice_bytes > 16 KiB ? 1 : 0). */
+#define P2G_BATCH_CLASSES 8
+
+/* Batch autotuner: times each form valid for a class on one synthetic
+ * problem of that class (8, 64, 160 or 420 outputs of ten times as many
+ * inputs; slices of 8 KiB or 256 KiB; up to 64 copies of a small problem in
+ * one launch, as many as make about 2e9 symbol multiply-accumulates; best
+ * of `reps` launches of the persistent kernel after a warm-up) and keeps the
+ * fastest per class
+ * for this context's later batches.  forms_out / ms_out (optional,
+ * P2G_BATCH_CLASSES entries) receive the chosen forms and their times. */
+int p2g_batch_autotune(p2g_ctx *ctx, int reps, int *forms_out, float *ms_out);
+/* Pins the form per class (P2G_BATCH_CLASSES entries; -1, or forms NULL,
+ * restores the heuristic: small tables up to 24 outputs, paired above 104,
+ * wide between).  P2G_EINVAL for the small form on a class above 24
+ * outputs. */
+int p2g_batch_set_forms(p2g_ctx *ctx, const int *forms);
+
 /* Size of the fixed device scratch array behind p2g_encode_noalloc. */
 #define P2G_NOALLOC_SCRATCH_BYTES (64u << 20)
 

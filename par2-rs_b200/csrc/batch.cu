@@ -199,7 +199,146 @@ struct Prob {
     // records: par2 (consts/exps offsets) or matrix (coeff device pointer)
     size_t consts_off, exps_off;
     const uint16_t *coeff;  // device
+    int form;               // tile form of the persistent kernel (BatchForm)
 };
+
+// The tile form for a problem: the context's tuned form for its class if
+// there is one, else small tables up to 24 outputs, the paired form above
+// 104 (one table build per input serves up to 208 outputs) and the 8 + 8
+// tables over 1024-symbol tiles between.
+// Input splits of an item of `unit` cost when the queue aims at items of
+// `target` cost (whole aligned words: S % 4 == 0; at least 16 inputs each).
+int split_for(double unit, double target, int nin, size_t S)
+{
+    if (unit <= target || S % 4)
+        return 1;
+    const double ns = std::min<double>({std::ceil(unit / target), std::max(1.0, nin / 16.0), 64.0});
+    return std::max(1, static_cast<int>(ns));
+}
+
+int form_for(const p2g_ctx *ctx, int nout, size_t S)
+{
+    const int f = ctx->batch_forms[batch_class(nout, S)];
+    if (batch_form_valid(f, nout))
+        return f;
+    return nout <= 24 ? kFormSmall : nout > 104 ? kFormPaired : kFormWide;
+}
+
+// Times each valid form of the persistent kernel on `copies` synthetic
+// problems of class `cls` in one launch (nin x nout each, slices of S bytes,
+// shared sources and coefficients from a random matrix, outputs of their own,
+// XORed into) and returns the fastest in *best_form.
+int tune_class(p2g_ctx *ctx, int cls, int nin, int nout, size_t S, int copies, int reps,
+               cudaEvent_t e0, cudaEvent_t e1, int *best_form, float *best_ms)
+{
+    cudaStream_t st = ctx->stream;
+    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    const int T = static_cast<int>((S + 2047) / 2048);
+    P2G_TRY(ctx->in_copy.ensure(S * nin));
+    P2G_TRY(ctx->out_copy.ensure(S * nout * copies));
+    P2G_TRY(ctx->coeffs.ensure(static_cast<size_t>(nin) * nout * 2 + 16));
+    P2G_TRY(ctx->recs.ensure(static_cast<size_t>(nin) * nout * kRecordWordsSmall * 4));
+    P2G_TRY(ctx->planes.ensure(static_cast<size_t>(nin) * T * 2048));
+    P2G_TRY(fill_synthetic(st, ctx->in_copy.p, S * nin, 11u + cls));
+    P2G_TRY(fill_synthetic(st, ctx->coeffs.p, (static_cast<size_t>(nin) * nout * 2) & ~size_t(3),
+                           29u + cls));
+    std::vector<const uint8_t *> sp(nin);
+    std::vector<uint8_t *> dv(static_cast<size_t>(nout) * copies);
+    for (int i = 0; i < nin; ++i)
+        sp[i] = ctx->in_copy.as<uint8_t>() + i * S;
+    for (size_t o = 0; o < dv.size(); ++o)
+        dv[o] = ctx->out_copy.as<uint8_t>() + o * S;
+    *best_form = -1;
+    *best_ms = 1e30f;
+    for (int f = 0; f < kBatchForms; ++f) {
+        if (!batch_form_valid(f, nout))
+            continue;
+        const int blk = batch_block(f);
+        const int nblk = (nout + blk - 1) / blk;
+        const int tiles = static_cast<int>((S + batch_tile_bytes(f) - 1) / batch_tile_bytes(f));
+        const double unit = static_cast<double>(nin) * batch_item_cost(f, std::min(nout, blk));
+        const double target = std::max(1.0, unit * tiles * nblk * copies / (4.0 * sms));
+        const int ns = split_for(unit, target, nin, S);
+        std::vector<BatchItem> items;
+        for (int c = 0; c < copies; ++c)
+            for (int t = 0; t < tiles; ++t)
+                for (int ob = 0; ob < nblk; ++ob)
+                    for (int x = 0; x < ns; ++x)
+                        items.push_back(BatchItem{c, t, ob, x});
+        // upload image: pointer tables, counter + abort word, problem tables, items
+        Image img;
+        const size_t src_off = img.put(sp.data(), nin * sizeof(void *));
+        const size_t dst_off = img.put(dv.data(), dv.size() * sizeof(void *));
+        const size_t ctr_off = img.put(nullptr, 64);
+        const size_t pl_off = img.put(nullptr, sizeof(PlanesProb));
+        const size_t rc_off = img.put(nullptr, sizeof(RecProb));
+        const size_t bp_off = img.put(nullptr, copies * sizeof(BatchProb));
+        const size_t it_off = img.put(items.data(), items.size() * sizeof(BatchItem));
+        P2G_TRY(ctx->params.ensure(img.bytes.size()));
+        uint8_t *base = ctx->params.as<uint8_t>();
+        PlanesProb pp{};
+        pp.src = reinterpret_cast<const uint8_t *const *>(base + src_off);
+        pp.planes = ctx->planes.as<uint32_t>();
+        pp.S = S;
+        pp.nin = nin;
+        pp.T = T;
+        RecProb rp{};
+        rp.coeff = ctx->coeffs.as<uint16_t>();
+        rp.recs = ctx->recs.as<uint32_t>();
+        rp.nin = nin;
+        rp.nout = nout;
+        rp.small = f == kFormSmall;
+        BatchProb bp{};
+        bp.planes = pp.planes;
+        bp.recs = rp.recs;
+        bp.dst = reinterpret_cast<uint8_t *const *>(base + dst_off);
+        bp.S = S;
+        bp.nin = nin;
+        bp.nout = nout;
+        bp.T = T;
+        bp.nblk = nblk;
+        bp.nsplit = ns;
+        bp.mode = 1;
+        bp.form = f;
+        memcpy(img.bytes.data() + pl_off, &pp, sizeof pp);
+        memcpy(img.bytes.data() + rc_off, &rp, sizeof rp);
+        for (int c = 0; c < copies; ++c) {
+            bp.dst = reinterpret_cast<uint8_t *const *>(base + dst_off) +
+                     static_cast<size_t>(c) * nout;
+            memcpy(img.bytes.data() + bp_off + c * sizeof bp, &bp, sizeof bp);
+        }
+        // a pageable source: the copy has read it when the call returns
+        P2G_CUDA(cudaMemcpyAsync(base, img.bytes.data(), img.bytes.size(), cudaMemcpyHostToDevice, st));
+        P2G_CUDA(cudaMemsetAsync(base + ctr_off, 0, 64, st));
+        P2G_TRY(batch_planes(st, reinterpret_cast<const PlanesProb *>(base + pl_off), 1,
+                             static_cast<unsigned long long>(nin) * T * 32));
+        P2G_TRY(batch_records(st, ctx->d_log, ctx->d_exp,
+                              reinterpret_cast<const RecProb *>(base + rc_off), 1,
+                              static_cast<unsigned long long>(nin) * nout));
+        int *counter = reinterpret_cast<int *>(base + ctr_off);
+        const volatile int *abort_word = counter + 8;
+        const int grid = static_cast<int>(std::min<size_t>(items.size(), sms));
+        float t_best = 1e30f;
+        for (int r = 0; r <= reps; ++r) {  // the first launch warms up
+            P2G_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
+            P2G_CUDA(cudaEventRecord(e0, st));
+            P2G_TRY(batch_muladd(st, grid, reinterpret_cast<const BatchProb *>(base + bp_off),
+                                 reinterpret_cast<const BatchItem *>(base + it_off),
+                                 static_cast<int>(items.size()), counter, abort_word));
+            P2G_CUDA(cudaEventRecord(e1, st));
+            P2G_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            P2G_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (r > 0)
+                t_best = std::min(t_best, ms);
+        }
+        if (t_best < *best_ms) {
+            *best_ms = t_best;
+            *best_form = f;
+        }
+    }
+    return P2G_OK;
+}
 
 }  // namespace
 
@@ -472,13 +611,15 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
     }
     // ---- scratch and work tables per phase ----
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    for (Prob &p : probs)
+        p.form = form_for(ctx, p.nout, p.S);
     size_t plane_need = 0, rec_need = 0;
     for (int x = 0; x < 2; ++x) {
         size_t pl = 0, rc = 0;
         for (const Prob &p : probs)
             if (p.phase == x) {
                 pl += static_cast<size_t>(p.nin) * ((p.S + 2047) / 2048) * 2048;
-                rc += static_cast<size_t>(p.nin) * p.nout * kRecordWords * 4;
+                rc += static_cast<size_t>(p.nin) * p.nout * batch_record_words(p.form) * 4;
             }
         plane_need = std::max(plane_need, pl);
         rec_need = std::max(rec_need, rc);
@@ -511,10 +652,13 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
         unsigned long long pl_first = 0, rc_first = 0;
         double total_cost = 0;
         for (const Prob &p : probs)
-            if (p.phase == x)
-                total_cost += static_cast<double>(p.nin) * ((p.S + 2047) / 2048) *
-                              ((p.nout + kBatchBlock - 1) / kBatchBlock) *
-                              (512.0 + 32.0 * std::min(p.nout, kBatchBlock));
+            if (p.phase == x) {
+                const int blk = batch_block(p.form);
+                const size_t tb = batch_tile_bytes(p.form);
+                total_cost += static_cast<double>(p.nin) * ((p.S + tb - 1) / tb) *
+                              ((p.nout + blk - 1) / blk) *
+                              batch_item_cost(p.form, std::min(p.nout, blk));
+            }
         const double target = std::max(1.0, total_cost / (4.0 * sms));
         for (size_t pi = 0; pi < probs.size(); ++pi) {
             const Prob &p = probs[pi];
@@ -538,6 +682,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
             rp.consts = p.coeff ? nullptr : reinterpret_cast<const uint16_t *>(p.consts_off);
             rp.exps = p.coeff ? nullptr : reinterpret_cast<const uint32_t *>(p.exps_off);
             rp.recs = reinterpret_cast<uint32_t *>(b->recs.as<uint8_t>() + rc_off);
+            rp.small = p.form == kFormSmall;
             P.rc.push_back(rp);
             BatchProb bp{};
             bp.planes = pp.planes;
@@ -547,18 +692,18 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
             bp.nin = p.nin;
             bp.nout = p.nout;
             bp.T = T;
-            bp.nblk = (p.nout + kBatchBlock - 1) / kBatchBlock;
+            const int blk = batch_block(p.form);
+            bp.nblk = (p.nout + blk - 1) / blk;
             bp.mode = p.mode;
+            bp.form = p.form;
             const double unit = static_cast<double>(p.nin) *
-                                (512.0 + 32.0 * std::min(p.nout, kBatchBlock));
-            int ns = 1;
-            if (unit > target && p.S % 4 == 0)
-                ns = static_cast<int>(std::min<double>({std::ceil(unit / target),
-                                                        std::max(1.0, p.nin / 16.0), 64.0}));
-            bp.nsplit = std::max(1, ns);
+                                batch_item_cost(p.form, std::min(p.nout, blk));
+            bp.nsplit = split_for(unit, target, p.nin, p.S);
             const int bpi = static_cast<int>(P.bp.size());
             P.bp.push_back(bp);
-            for (int t = 0; t < T; ++t)
+            const int tiles = static_cast<int>((p.S + batch_tile_bytes(p.form) - 1) /
+                                               batch_tile_bytes(p.form));
+            for (int t = 0; t < tiles; ++t)
                 for (int ob = 0; ob < bp.nblk; ++ob)
                     for (int sp = 0; sp < bp.nsplit; ++sp)
                         P.items.push_back(BatchItem{bpi, t, ob, sp});
@@ -572,7 +717,7 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
                 }
             }
             pl_off += static_cast<size_t>(p.nin) * T * 2048;
-            rc_off += static_cast<size_t>(p.nin) * p.nout * kRecordWords * 4;
+            rc_off += static_cast<size_t>(p.nin) * p.nout * batch_record_words(p.form) * 4;
             pl_first += static_cast<unsigned long long>(p.nin) * T * 32;
             rc_first += static_cast<unsigned long long>(p.nin) * p.nout;
         }
@@ -581,8 +726,9 @@ int p2g_batch_create(p2g_ctx *ctx, p2g_job *jobs, size_t njobs, uint32_t flags, 
         for (size_t i = 0; i < P.items.size(); ++i) {
             const BatchItem &it = P.items[i];
             const BatchProb &bp = P.bp[it.prob];
-            const int nb = std::min(kBatchBlock, bp.nout - it.ob * kBatchBlock);
-            cost[i] = static_cast<double>(bp.nin) / bp.nsplit * (512.0 + 32.0 * nb);
+            const int blk = batch_block(bp.form);
+            const int nb = std::min(blk, bp.nout - it.ob * blk);
+            cost[i] = static_cast<double>(bp.nin) / bp.nsplit * batch_item_cost(bp.form, nb);
         }
         std::vector<size_t> order(P.items.size());
         for (size_t i = 0; i < order.size(); ++i)
@@ -831,6 +977,71 @@ int p2g_batch_destroy(p2g_batch *b)
     std::lock_guard<std::mutex> lock(b->ctx->mu);
     batch_free(b);
     return P2G_OK;
+}
+
+int p2g_batch_set_forms(p2g_ctx *ctx, const int *forms)
+{
+    clear_error();
+    if (!ctx) {
+        set_error("p2g_batch_set_forms: null context");
+        return P2G_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    for (int c = 0; c < 8; ++c) {
+        const int f = forms ? forms[c] : -1;
+        if (f != -1 && !batch_form_valid(f, c < 2 ? 24 : 25)) {
+            set_error("p2g_batch_set_forms: form %d is not valid for class %d", f, c);
+            return P2G_EINVAL;
+        }
+    }
+    for (int c = 0; c < 8; ++c)
+        ctx->batch_forms[c] = forms ? forms[c] : -1;
+    return P2G_OK;
+}
+
+int p2g_batch_autotune(p2g_ctx *ctx, int reps, int *forms_out, float *ms_out)
+{
+    clear_error();
+    if (!ctx) {
+        set_error("p2g_batch_autotune: null context");
+        return P2G_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    P2G_CUDA(cudaSetDevice(ctx->device));
+    reps = std::max(1, reps);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0)
+            cudaEventDestroy(e0);
+        (void)cudaGetLastError();
+        set_error("p2g_batch_autotune: cudaEventCreate failed");
+        return P2G_ECUDA;
+    }
+    // representative outputs per class pair, ten inputs per output (a set
+    // of 10 % redundancy)
+    static const int kOut[4] = {8, 64, 160, 420};
+    int rc = P2G_OK;
+    for (int c = 0; c < 8 && rc == P2G_OK; ++c) {
+        const int nout = kOut[c / 2];
+        const size_t S = (c & 1) ? (256u << 10) : (8u << 10);
+        int form = -1;
+        float ms = 0.f;
+        // as many problems in one launch as give about 2e9 symbol
+        // multiply-accumulates (small sets run many to a batch), at most 64
+        const double macs = 10.0 * nout * nout * (S / 2.0);
+        const int copies = static_cast<int>(std::min(64.0, std::max(1.0, std::ceil(2e9 / macs))));
+        rc = tune_class(ctx, c, 10 * nout, nout, S, copies, reps, e0, e1, &form, &ms);
+        if (rc == P2G_OK) {
+            ctx->batch_forms[c] = form;
+            if (forms_out)
+                forms_out[c] = form;
+            if (ms_out)
+                ms_out[c] = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
 }
 
 }  // extern "C"

@@ -59,6 +59,9 @@ inline PlanKey plan_key(int nin, int nout, size_t S) { return PlanKey(nin, nout,
 struct p2g_ctx {
     // tuned plans (p2g_autotune); choose_plan falls back to a heuristic
     std::map<p2g::PlanKey, p2g::MuladdPlan> plans;
+    // tile form of the persistent batch kernel per problem class
+    // (p2g_batch_autotune / p2g_batch_set_forms); -1: the heuristic's
+    int batch_forms[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
     int device = 0;
     int sm_count = 0;
     cudaStream_t own_stream = nullptr;  // created with the context

@@ -754,9 +754,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
 
 // Persistent form for batches of independent problems: one CTA per SM takes
 // items (problem, tile, output block, input split) from a queue ordered
-// longest first and runs each as muladd_bitsliced would.
-template <int WARPS, int EREG, int PSPLIT>
-__global__ void __launch_bounds__(WARPS * 32, 1)
+// longest first and runs each in its problem's form as muladd_bitsliced /
+// muladd_paired would.
+__global__ void __launch_bounds__(kBatchWarps * 32, 1)
     muladd_persistent(const BatchProb *__restrict__ probs, const BatchItem *__restrict__ items,
                       int nitems, int *__restrict__ counter, const volatile int *abort)
 {
@@ -780,9 +780,16 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
         const int i0 = static_cast<int>(static_cast<long long>(p.nin) * item.split / p.nsplit);
         const int i1 =
             static_cast<int>(static_cast<long long>(p.nin) * (item.split + 1) / p.nsplit);
-        muladd_item<WARPS, EREG, PSPLIT>(smem, p.planes, p.recs, p.nin, p.nout, p.T, item.t,
-                                         item.ob, i0, i1, p.dst, p.S,
-                                         p.nsplit > 1 ? 2 : p.mode);
+        const int smode = p.nsplit > 1 ? 2 : p.mode;
+        if (p.form == kFormPaired)
+            muladd_item_paired<kBatchWarps, 13, 2>(smem, p.planes, p.recs, p.nout, p.T, item.t,
+                                                   item.ob, i0, i1, p.dst, p.S, smode);
+        else if (p.form == kFormSmall)
+            muladd_item<kBatchWarps, 3, 1, true>(smem, p.planes, p.recs, p.nin, p.nout, p.T,
+                                                 item.t, item.ob, i0, i1, p.dst, p.S, smode);
+        else
+            muladd_item<kBatchWarps, 13, 1>(smem, p.planes, p.recs, p.nin, p.nout, p.T, item.t,
+                                            item.ob, i0, i1, p.dst, p.S, smode);
         __syncthreads();
     }
 }
@@ -1088,6 +1095,15 @@ __global__ void fill_pattern(uint32_t *p, size_t words, uint32_t seed)
     }
 }
 
+int fill_synthetic(cudaStream_t st, void *p, size_t bytes, uint32_t seed)
+{
+    if (bytes < 4)
+        return P2G_OK;
+    fill_pattern<<<1024, 256, 0, st>>>(static_cast<uint32_t *>(p), bytes / 4, seed);
+    P2G_CUDA(cudaGetLastError());
+    return P2G_OK;
+}
+
 int muladd_autotune(p2g_ctx *ctx, int nin, int nout, size_t S, int reps, MuladdPlan *best,
                     float *best_ms, int *tried)
 {
@@ -1301,7 +1317,7 @@ __global__ void batch_records_kernel(const RecProb *__restrict__ probs, int np,
         else
             c = gexp[static_cast<uint32_t>((static_cast<uint64_t>(glog[base]) * e) % 65535u)];
     }
-    write_record(p.recs, local, c, false);  // the batch kernel reads the 8 + 8 form
+    write_record(p.recs, local, c, p.small != 0);
 }
 
 __global__ void batch_zero_kernel(uint8_t *const *__restrict__ ptrs,
@@ -1383,20 +1399,29 @@ int batch_copy(cudaStream_t st, const uint8_t *const *src, uint8_t *const *dst,
     return P2G_OK;
 }
 
+// Shared memory of the persistent kernel: the largest of its forms'.
+static size_t batch_smem_bytes()
+{
+    MuladdPlan w, sm, pr;
+    w.warps = sm.warps = pr.warps = kBatchWarps;
+    w.ereg = 13;
+    sm.ereg = 3;
+    sm.small = true;
+    pr.ereg = 13;
+    pr.paired = true;
+    pr.stage = 2;
+    return std::max({smem_bytes(w), smem_bytes(sm), smem_bytes(pr)});
+}
+
 int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchItem *items,
                  int nitems, int *counter, const volatile int *abort)
 {
     if (nitems <= 0)
         return P2G_OK;
-    constexpr int W = kBatchWarps, E = kBatchEreg;
-    MuladdPlan p;
-    p.warps = W;
-    p.ereg = E;
-    const size_t smem = smem_bytes(p);
-    auto fn = muladd_persistent<W, E, 1>;
-    P2G_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem = batch_smem_bytes();
+    P2G_CUDA(cudaFuncSetAttribute(muladd_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
-    fn<<<grid, W * 32, smem, st>>>(probs, items, nitems, counter, abort);
+    muladd_persistent<<<grid, kBatchWarps * 32, smem, st>>>(probs, items, nitems, counter, abort);
     P2G_CUDA(cudaGetLastError());
     return P2G_OK;
 }

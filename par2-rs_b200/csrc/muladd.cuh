@@ -19,20 +19,59 @@ inline size_t record_bytes(size_t nin, int nout)
     return nin * static_cast<size_t>(nout) * record_words(nout) * 4;
 }
 
+// Tile forms of the persistent batch kernel, chosen per problem: the 8 + 8
+// tables over 1024-symbol tiles (8 warps x 13 outputs, 104 per item), the
+// small-output tables (8 warps x 3, 24 per item) and the paired form over
+// 512-symbol tiles (8 warps x 13 output pairs, 208 per item, two inputs per
+// barrier).
+enum BatchForm : int { kFormWide = 0, kFormSmall = 1, kFormPaired = 2, kBatchForms = 3 };
+inline int batch_block(int form)
+{
+    return form == kFormSmall ? 24 : form == kFormPaired ? 208 : 104;
+}
+// column bytes one item covers
+inline size_t batch_tile_bytes(int form) { return form == kFormPaired ? 1024 : 2048; }
+inline int batch_record_words(int form)
+{
+    return form == kFormSmall ? kRecordWordsSmall : kRecordWords;
+}
+// Shared-memory wavefronts one input of an item of nb outputs costs: table
+// rows built plus plane reads, then table reads and record loads per output.
+inline double batch_item_cost(int form, int nb)
+{
+    if (form == kFormSmall)
+        return 144.0 + 50.0 * nb;
+    if (form == kFormPaired)
+        return 320.0 + 17.0 * nb;
+    return 576.0 + 34.0 * nb;
+}
+// The problem classes the batch autotuner keys on: outputs 1-24, 25-104,
+// 105-208, more; slices up to 16 KiB or larger.
+inline int batch_class(int nout, size_t S)
+{
+    const int c = nout <= 24 ? 0 : nout <= 104 ? 1 : nout <= 208 ? 2 : 3;
+    return 2 * c + (S > (16u << 10) ? 1 : 0);
+}
+// A form's validity for a problem: the small tables take at most 24 outputs.
+inline bool batch_form_valid(int form, int nout)
+{
+    return form >= 0 && form < kBatchForms && (form != kFormSmall || nout <= 24);
+}
+
 // One multiply-accumulate problem of a batch (device-resident description).
 struct BatchProb {
     const uint32_t *planes;  // [nin][T][512]
-    const uint32_t *recs;    // [nin][nout][8] (the batch kernel uses the 8 + 8 tables)
+    const uint32_t *recs;    // [nin][nout][batch_record_words(form)]
     uint8_t *const *dst;     // nout device pointers
     size_t S;                // bytes per slice
-    int nin, nout, T, nblk, nsplit, mode;
+    int nin, nout, T, nblk, nsplit, mode, form;
 };
-// One work item of a batch: (problem, column tile, output block, input split).
+// One work item of a batch: (problem, column tile of the problem's form,
+// output block, input split).
 struct BatchItem {
     int prob, t, ob, split;
 };
-// Shape of the persistent batch kernel: 8 warps x 13 outputs (104 per block).
-constexpr int kBatchWarps = 8, kBatchEreg = 13, kBatchBlock = kBatchWarps * kBatchEreg;
+constexpr int kBatchWarps = 8;
 
 // Bit-plane conversion of one problem of a batch; `first` is the problem's
 // first thread in the batched grid (nin * T * 32 threads each).
@@ -51,6 +90,7 @@ struct RecProb {
     const uint16_t *coeff;
     uint32_t *recs;
     int nin, nout;
+    int small;  // small-output (24-word) records
     unsigned long long first;
 };
 
@@ -60,8 +100,8 @@ int batch_records(cudaStream_t st, const uint16_t *glog, const uint16_t *gexp, c
 int batch_zero(cudaStream_t st, uint8_t *const *ptrs, const unsigned long long *bytes, int n);
 int batch_copy(cudaStream_t st, const uint8_t *const *src, uint8_t *const *dst,
                const unsigned long long *bytes, int n);
-// The persistent kernel over `nitems` items (longest first) with `grid` CTAs;
-// *counter must be zero.  A CTA takes no further item once it has seen the
+// The persistent kernel over `nitems` items (longest first) with `grid` CTAs,
+// each item run in its problem's form; *counter must be zero.  A CTA takes no further item once it has seen the
 // device word *abort non-zero (polled every 4th item).
 int batch_muladd(cudaStream_t st, int grid, const BatchProb *probs, const BatchItem *items,
                  int nitems, int *counter, const volatile int *abort);
@@ -78,6 +118,9 @@ bool plan_valid(const MuladdPlan &p, int nin, int nout, size_t slice_bytes);
 // The compiled (warps, outputs per group, warps per group) shapes; returns
 // their number.
 int muladd_variants(int *warps, int *eregs, int *psplits, int cap);
+
+// Deterministic pseudo-random words over bytes / 4 words at p (device).
+int fill_synthetic(cudaStream_t st, void *p, size_t bytes, uint32_t seed);
 
 // Times every candidate plan for (nin, nout, S) on synthetic data in the
 // context's scratch, caches the fastest in ctx->plans and returns it.

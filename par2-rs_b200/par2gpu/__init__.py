@@ -69,8 +69,14 @@ SIGNATURES = [
     ("p2g_batch_wait", _I, [_P]),
     ("p2g_batch_cancel", _I, [_P]),
     ("p2g_batch_destroy", _I, [_P]),
+    ("p2g_batch_autotune", _I, [_P, _I, _P, _P]),
+    ("p2g_batch_set_forms", _I, [_P, _P]),
 ]
 JOB_CREATE, JOB_REPAIR, JOB_VERIFY = 1, 2, 3
+# tile forms of the persistent batch kernel and the problem classes they are
+# chosen for (par2gpu.h P2G_FORM_*, P2G_BATCH_CLASSES)
+FORM_WIDE, FORM_SMALL, FORM_PAIRED = 0, 1, 2
+BATCH_CLASSES = 8
 BATCH_GRAPH = 0x2
 
 
@@ -250,6 +256,25 @@ class Context:
         p = Plan()
         check(lib().p2g_autotune(self.h, nin, nout, slice_bytes, reps, ctypes.byref(p)))
         return p
+
+    def batch_autotune(self, reps=2):
+        """Time the persistent batch kernel's tile forms per problem class and
+        keep the fastest for this context's batches; returns (forms, ms), one
+        entry per class (FORM_WIDE / FORM_SMALL / FORM_PAIRED)."""
+        forms = np.zeros(BATCH_CLASSES, np.int32)
+        ms = np.zeros(BATCH_CLASSES, np.float32)
+        check(lib().p2g_batch_autotune(self.h, reps, forms.ctypes.data, ms.ctypes.data))
+        return [int(f) for f in forms], [float(t) for t in ms]
+
+    def batch_set_forms(self, forms=None):
+        """Pin the batch kernel's form per class (None or -1: the heuristic)."""
+        if forms is None:
+            check(lib().p2g_batch_set_forms(self.h, None))
+            return
+        f = np.ascontiguousarray(forms, np.int32)
+        if f.size != BATCH_CLASSES:
+            raise ValueError(f"batch_set_forms takes {BATCH_CLASSES} forms")
+        check(lib().p2g_batch_set_forms(self.h, f.ctypes.data))
 
     def set_plan(self, nin, nout, slice_bytes, warps, outputs_per_group, output_blocks,
                  input_splits=1, warps_per_group=1, tile_symbols=1024, inputs_per_stage=1):

@@ -45,11 +45,62 @@ def make_set(rng, k, S, r):
 
 
 def test_mixed_batch_matches_oracle(ctx):
-    import torch
+    """Default forms: small tables for 1-24 outputs, the 8 + 8 tables for
+    25-104, the paired form above 104 -- all three in one persistent run."""
+    ctx.batch_set_forms(None)
+    mixed_batch_roundtrip(ctx, 41)
 
+
+# Forms pinned per class (classes 0-1: 1-24 outputs, 2-3: 25-104, 4-5: 105-208,
+# 6-7: more); every valid form runs every problem of the mixed batch.
+FORM_MAPS = {
+    "wide": [0] * 8,
+    "paired": [2] * 8,
+    "small_then_paired": [1, 1, 2, 2, 2, 2, 2, 2],
+    "small_then_wide": [1, 1, 0, 0, 0, 0, 0, 0],
+    "by_slice_size": [1, 0, 0, 2, 2, 0, 0, 2],
+}
+
+
+@pytest.mark.parametrize("name", sorted(FORM_MAPS))
+def test_mixed_batch_in_pinned_forms(ctx, name):
+    ctx.batch_set_forms(FORM_MAPS[name])
+    try:
+        mixed_batch_roundtrip(ctx, 43)
+    finally:
+        ctx.batch_set_forms(None)
+
+
+def test_batch_autotune_picks_valid_forms_and_keeps_parity(ctx):
     import par2gpu
 
-    rng = np.random.default_rng(41)
+    forms, ms = ctx.batch_autotune(reps=1)
+    assert len(forms) == par2gpu.BATCH_CLASSES
+    for c, f in enumerate(forms):
+        assert f in (par2gpu.FORM_WIDE, par2gpu.FORM_PAIRED) or (f == par2gpu.FORM_SMALL and c < 2)
+        assert 0 < ms[c] < 1e4
+    try:
+        mixed_batch_roundtrip(ctx, 44)
+    finally:
+        ctx.batch_set_forms(None)
+
+
+def test_set_forms_rejects_small_form_above_24_outputs(ctx):
+    import par2gpu
+
+    with pytest.raises(par2gpu.Par2GpuError):
+        ctx.batch_set_forms([1] * 8)
+    with pytest.raises(ValueError):
+        ctx.batch_set_forms([0] * 7)
+    ctx.batch_set_forms(None)
+
+
+def mixed_batch_roundtrip(ctx, seed):
+    """Creates of 1-110 outputs, repairs (single-CTA, blocked and host
+    inverses) and a verify in one batch; every job equals the oracle's."""
+    import par2gpu
+
+    rng = np.random.default_rng(seed)
     shapes = [(5, 4096, 1), (60, 6144 + 64, 13), (300, 2048, 3), (17, 16384, 40),
               (200, 8192, 110), (1, 64, 1), (33, 2050, 7)]
     jobs, checks = [], []
