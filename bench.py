@@ -312,9 +312,11 @@ def run_ours(args, rank, world):
     macs = k * r * (S // 2)
     int_ops = 2.0 * macs
     alg_bytes = (k + r) * S
+    # the heuristic plan takes the paired form above 104 outputs
+    paired = (plan["tile_symbols"] == 512) if plan else r > 104
     roofline = {
         "bound": "int",
-        "kernel": "muladd_bitsliced",
+        "kernel": "muladd_paired" if paired else "muladd_bitsliced",
         "achieved": int_ops / t_kernel / 1e12,
         "peak": (int_peak or 0) / 1e12,
         "unit": "Tops/s (2 LOP3 per GF(2^16) symbol MAC)",
