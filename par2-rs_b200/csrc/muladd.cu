@@ -539,10 +539,10 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
     constexpr int RING = pair_ring_slots(STAGE);
     uint32_t *tab = reinterpret_cast<uint32_t *>(smem);
     uint8_t *ring = smem + 2 * STAGE * TW * 4;
-    // ring slot of input i (RING = 4 needs no reference to i0)
-    auto slot = [&](int i) {
-        return ring + (RING == 4 ? (i & 3) : (i - i0) % RING) * SLOT;
-    };
+    // ring slot of input i (RING is a power of two: any RING consecutive
+    // inputs take distinct slots)
+    static_assert((RING & (RING - 1)) == 0, "ring slots: a power of two");
+    auto slot = [&](int i) { return ring + (i & (RING - 1)) * SLOT; };
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
