@@ -178,12 +178,15 @@ def test_repair_matches_oracle(ctx, k, S, m):
     assert np.array_equal(got, src[missing])
 
 
-def test_repair_from_host_buffers_in_upload_groups(ctx):
-    """Host present slices (2041 of them, ragged 2050-byte slices) go up in 16
-    groups while the decode matrix forms and the earlier groups accumulate;
-    the rebuilt slices equal the oracle's."""
-    rng = np.random.default_rng(77)
-    k, S, m = 2048, 2050, 7
+@pytest.mark.parametrize("m", [7, 40])
+def test_repair_from_host_buffers_in_upload_groups(ctx, m):
+    """Host present slices (2048 - m of them, ragged 2050-byte slices) go up
+    in 16 groups while the decode matrix forms and the earlier groups
+    accumulate; the rebuilt slices equal the oracle's.  m = 7 runs the
+    small-output records (24 words), m = 40 the 8 + 8 records (8 words), so
+    both record strides pass through the per-group offsets."""
+    rng = np.random.default_rng(77 + m)
+    k, S = 2048, 2050
     src = rng.integers(0, 256, (k, S), dtype=np.uint8)
     exps = np.arange(m, dtype=np.uint32)
     rec = ctx.encode_array(src, exps)
