@@ -34,12 +34,22 @@
 // for the recorded work that uses it; an unprepared destination makes the
 // call synchronous (pending work is run first and a prepared source is read
 // back from its mirror).
+//
+// Cost per call: the callers make one multiply-accumulate call per
+// (destination, source) pair from many threads (par2_rs.rs:832-866), so a
+// recorded product takes one uncontended lock: the mirror map and the
+// pending products are split over shards, a thread records into its own
+// shard, and prepare / finish / flush take every shard.  Prepare copies the
+// caller's buffer into the pinned staging ring with helper threads, and
+// device blocks of retired mirrors are kept for reuse once the work that
+// used them has completed.
 #include <string.h>
 
 #include <algorithm>
-#include <map>
+#include <atomic>
+#include <condition_variable>
 #include <mutex>
-#include <shared_mutex>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -61,9 +71,9 @@ struct Mirror {
     uint8_t *dev = nullptr;
     size_t bytes = 0;
     uintptr_t host = 0;  // the address it mirrors while current
-    int refs = 0;        // recorded products that read or write it
+    int refs = 0;        // recorded products that read or write it (atomic)
     bool current = false;
-    bool dst = false;    // written by recorded products
+    bool dst = false;    // written by recorded products (atomic)
 };
 
 struct Product {
@@ -72,19 +82,106 @@ struct Product {
     uint16_t c;
 };
 
+constexpr int kShards = 16;
+
+// One lock of the sharded map lock, with the products recorded under it.
+struct alignas(64) Shard {
+    std::mutex mu;
+    std::vector<Product> pending;
+    double macs = 0;
+    size_t src_bytes = 0;
+};
+
+// A device block of a retired mirror, reusable once `ev` has completed.
+struct FreeBlock {
+    uint8_t *dev;
+    size_t bytes;
+    cudaEvent_t ev;
+};
+constexpr size_t kMaxFreeBytes = size_t(2) << 30;
+
+// Helper threads copying a staged chunk in parts: prepare must have read the
+// caller's buffer when it returns, and one thread copies ~13 GB/s.
+class CopyPool {
+  public:
+    explicit CopyPool(int helpers)
+    {
+        for (int i = 0; i < helpers; ++i)
+            th_.emplace_back([this] { loop(); });
+    }
+    ~CopyPool()
+    {
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread &t : th_)
+            t.join();
+    }
+    // n bytes from src to dst in up to helpers + 1 parts of at least 256 KiB
+    void copy(uint8_t *dst, const uint8_t *src, size_t n)
+    {
+        const size_t parts = std::min<size_t>(th_.size() + 1, std::max<size_t>(1, n >> 18));
+        if (parts <= 1) {
+            memcpy(dst, src, n);
+            return;
+        }
+        const size_t step = ((n + parts - 1) / parts + 63) & ~size_t(63);
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            dst_ = dst;
+            src_ = src;
+            n_ = n;
+            step_ = step;
+            parts_ = (n + step - 1) / step;
+            next_ = 1;
+            left_ = parts_ - 1;
+        }
+        cv_.notify_all();
+        memcpy(dst, src, std::min(step, n));  // part 0 on the calling thread
+        std::unique_lock<std::mutex> l(mu_);
+        done_.wait(l, [&] { return left_ == 0; });
+    }
+
+  private:
+    void loop()
+    {
+        std::unique_lock<std::mutex> l(mu_);
+        while (true) {
+            cv_.wait(l, [&] { return stop_ || next_ < parts_; });
+            if (stop_)
+                return;
+            const size_t p = next_++;
+            const size_t a = p * step_, b = std::min(n_, a + step_);
+            uint8_t *dst = dst_;
+            const uint8_t *src = src_;
+            l.unlock();
+            memcpy(dst + a, src + a, b - a);
+            l.lock();
+            if (--left_ == 0)
+                done_.notify_one();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    uint8_t *dst_ = nullptr;
+    const uint8_t *src_ = nullptr;
+    size_t n_ = 0, step_ = 0, parts_ = 0, next_ = 0, left_ = 0;
+    bool stop_ = false;
+};
+
 }  // namespace
 
 struct Deferred {
-    std::shared_mutex map_mu;  // mirrors, by_host
+    // The map lock: shard[j].mu for the recording threads of shard j, all
+    // of them (in index order) for everything that changes the map.
+    Shard shard[kShards];
     std::vector<Mirror> mirrors;
     std::vector<uint32_t> free_ids;
     std::unordered_map<uintptr_t, uint32_t> by_host;
-    int live_dsts = 0;  // current mirrors that recorded products write
-
-    std::mutex pend_mu;  // pending, pend_macs, pend_src_bytes, Mirror::refs
-    std::vector<Product> pending;
-    double pend_macs = 0;
-    size_t pend_src_bytes = 0;
+    int live_dsts = 0;  // current mirrors that recorded products write (atomic)
 
     std::mutex stage_mu;  // staging ring
     uint8_t *stage[kStageChunks] = {};
@@ -92,6 +189,12 @@ struct Deferred {
     int stage_next = 0;
     cudaEvent_t upload_ev = nullptr;  // after the latest upload on the copy stream
     bool uploads = false;
+    CopyPool *copier = nullptr;
+
+    // device blocks of retired mirrors (oldest first) and idle events
+    std::vector<FreeBlock> free_blocks;
+    size_t free_bytes = 0;
+    std::vector<cudaEvent_t> spare_events;
 
     // kernel parameters of a launch: pinned, two slots, each reused only after
     // the copy that read it has run
@@ -103,6 +206,33 @@ struct Deferred {
 };
 
 namespace {
+
+// The shard of the calling thread (threads take shards round robin).
+Shard &my_shard(Deferred *d)
+{
+    static std::atomic<unsigned> next{0};
+    thread_local unsigned mine = next.fetch_add(1) % kShards;
+    return d->shard[mine];
+}
+
+// Every shard's lock: the map may change.
+struct MapWriteLock {
+    Deferred *d;
+    bool held = true;
+    explicit MapWriteLock(Deferred *dd) : d(dd)
+    {
+        for (Shard &s : d->shard)
+            s.mu.lock();
+    }
+    void unlock()
+    {
+        if (held)
+            for (int j = kShards - 1; j >= 0; --j)
+                d->shard[j].mu.unlock();
+        held = false;
+    }
+    ~MapWriteLock() { unlock(); }
+};
 
 // ctx->mu held.
 int setup(p2g_ctx *ctx, Deferred *&out)
@@ -138,6 +268,12 @@ int setup(p2g_ctx *ctx, Deferred *&out)
             cudaMemPoolSetAttribute(d->pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
+    if (rc == P2G_OK) {
+        // helpers for the staging copies: up to 3 more threads, leaving the
+        // host's other cores to the caller's workers
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        d->copier = new CopyPool(static_cast<int>(std::min(3u, hw / 4)));
+    }
     if (rc != P2G_OK) {
         (void)cudaGetLastError();
         set_error("shuffle2x: setting up the device mirrors failed");
@@ -150,28 +286,72 @@ int setup(p2g_ctx *ctx, Deferred *&out)
     return P2G_OK;
 }
 
-// Frees mirror `id` on the compute stream (after every launch that used it
-// and every upload enqueued so far).  map_mu held exclusively.
+// Retires the device block of mirror `id`: it is kept for a later mirror
+// once every launch that used it and every upload enqueued so far have run
+// (an event on the compute stream after both); beyond kMaxFreeBytes of kept
+// blocks the oldest go back to the pool.  Map write-locked.
 int drop_mirror(p2g_ctx *ctx, Deferred *d, uint32_t id)
 {
     Mirror &m = d->mirrors[id];
     if (m.dev) {
         if (d->uploads)
             P2G_CUDA(cudaStreamWaitEvent(ctx->stream, d->upload_ev, 0));
-        P2G_CUDA(cudaFreeAsync(m.dev, ctx->stream));
+        cudaEvent_t ev = nullptr;
+        if (!d->spare_events.empty()) {
+            ev = d->spare_events.back();
+            d->spare_events.pop_back();
+        } else {
+            P2G_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        }
+        P2G_CUDA(cudaEventRecord(ev, ctx->stream));
+        d->free_blocks.push_back(FreeBlock{m.dev, m.bytes, ev});
+        d->free_bytes += m.bytes;
+        while (d->free_bytes > kMaxFreeBytes) {
+            const FreeBlock b = d->free_blocks.front();
+            d->free_blocks.erase(d->free_blocks.begin());
+            d->free_bytes -= b.bytes;
+            d->spare_events.push_back(b.ev);
+            P2G_CUDA(cudaFreeAsync(b.dev, ctx->stream));
+        }
     }
     m = Mirror{};
     d->free_ids.push_back(id);
     return P2G_OK;
 }
 
-// A new mirror of `bytes` holding a copy of host[0, bytes).  map_mu held
-// exclusively.
+// A device block of at least `bytes` for a new mirror: a kept block of the
+// same size whose last use has completed, else one from the pool (on the
+// copy stream, which uploads into it).  Map write-locked.
+int take_block(p2g_ctx *ctx, Deferred *d, size_t bytes, uint8_t *&dev)
+{
+    const size_t want = std::max<size_t>(bytes, 16);
+    for (size_t j = 0; j < d->free_blocks.size(); ++j) {
+        FreeBlock &b = d->free_blocks[j];
+        if (b.bytes != want)
+            continue;
+        const cudaError_t q = cudaEventQuery(b.ev);
+        if (q == cudaErrorNotReady) {
+            (void)cudaGetLastError();
+            continue;
+        }
+        P2G_CUDA(q);
+        dev = b.dev;
+        d->free_bytes -= b.bytes;
+        d->spare_events.push_back(b.ev);
+        d->free_blocks.erase(d->free_blocks.begin() + static_cast<long>(j));
+        return P2G_OK;
+    }
+    P2G_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&dev), want, d->pool,
+                                     ctx->copy_stream));
+    return P2G_OK;
+}
+
+// A new mirror of `bytes` holding a copy of host[0, bytes).  Map
+// write-locked.
 int new_mirror(p2g_ctx *ctx, Deferred *d, const void *host, size_t bytes, uint32_t &id)
 {
     uint8_t *dev = nullptr;
-    P2G_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&dev), std::max<size_t>(bytes, 16),
-                                     d->pool, ctx->copy_stream));
+    P2G_TRY(take_block(ctx, d, bytes, dev));
     {
         std::lock_guard<std::mutex> lock(d->stage_mu);
         const uint8_t *h = static_cast<const uint8_t *>(host);
@@ -180,7 +360,7 @@ int new_mirror(p2g_ctx *ctx, Deferred *d, const void *host, size_t bytes, uint32
             const int c = d->stage_next;
             d->stage_next = (c + 1) % kStageChunks;
             P2G_CUDA(cudaEventSynchronize(d->stage_ev[c]));
-            memcpy(d->stage[c], h + off, n);
+            d->copier->copy(d->stage[c], h + off, n);
             P2G_CUDA(cudaMemcpyAsync(dev + off, d->stage[c], n, cudaMemcpyHostToDevice,
                                      ctx->copy_stream));
             P2G_CUDA(cudaEventRecord(d->stage_ev[c], ctx->copy_stream));
@@ -202,7 +382,7 @@ int new_mirror(p2g_ctx *ctx, Deferred *d, const void *host, size_t bytes, uint32
 }
 
 // Makes mirror `id` no longer current; frees it when no recorded product
-// uses it.  map_mu held exclusively.
+// uses it.  Map write-locked (no product is being recorded).
 int retire(p2g_ctx *ctx, Deferred *d, uint32_t id)
 {
     Mirror &m = d->mirrors[id];
@@ -212,12 +392,7 @@ int retire(p2g_ctx *ctx, Deferred *d, uint32_t id)
             --d->live_dsts;
         m.current = false;
     }
-    int refs;
-    {
-        std::lock_guard<std::mutex> lock(d->pend_mu);
-        refs = m.refs;
-    }
-    return refs == 0 ? drop_mirror(ctx, d, id) : P2G_OK;
+    return m.refs == 0 ? drop_mirror(ctx, d, id) : P2G_OK;
 }
 
 // Pointer arrays and coefficient matrix of one launch in a parameter slot.
@@ -250,15 +425,18 @@ int launch_group(p2g_ctx *ctx, Deferred *d, const std::vector<uint8_t *> &srcs,
                       static_cast<int>(nout), bytes, ctx->recs.as<uint32_t>(), 1);
 }
 
-// Runs every recorded product.  ctx->mu and map_mu (exclusive) held.
+// Runs every recorded product.  ctx->mu held, map write-locked.
 int flush(p2g_ctx *ctx, Deferred *d)
 {
     std::vector<Product> work;
-    {
-        std::lock_guard<std::mutex> lock(d->pend_mu);
-        work.swap(d->pending);
-        d->pend_macs = 0;
-        d->pend_src_bytes = 0;
+    for (Shard &sh : d->shard) {
+        if (work.empty())
+            work.swap(sh.pending);
+        else
+            work.insert(work.end(), sh.pending.begin(), sh.pending.end());
+        sh.pending.clear();
+        sh.macs = 0;
+        sh.src_bytes = 0;
     }
     if (work.empty())
         return P2G_OK;
@@ -274,6 +452,7 @@ int flush(p2g_ctx *ctx, Deferred *d)
         return a.dst < b.dst;
     });
     int rc = P2G_OK;
+    std::vector<int> dix(d->mirrors.size(), -1);
     size_t g0 = 0;
     while (g0 < work.size() && rc == P2G_OK) {
         size_t g1 = g0;
@@ -281,13 +460,13 @@ int flush(p2g_ctx *ctx, Deferred *d)
             ++g1;
         const size_t off = work[g0].off, len = work[g0].len;
         // sources of the group in chunks of at most 65535, all destinations
-        std::map<uint32_t, size_t> dix;
-        for (size_t q = g0; q < g1; ++q)
-            dix.emplace(work[q].dst, 0);
+        // (dix: a destination mirror's row in the coefficient matrix)
         std::vector<uint8_t *> dsts;
-        for (auto &kv : dix) {
-            kv.second = dsts.size();
-            dsts.push_back(d->mirrors[kv.first].dev + off * 2);
+        for (size_t q = g0; q < g1; ++q) {
+            if (dix[work[q].dst] < 0) {
+                dix[work[q].dst] = static_cast<int>(dsts.size());
+                dsts.push_back(d->mirrors[work[q].dst].dev + off * 2);
+            }
         }
         size_t q = g0;
         while (q < g1 && rc == P2G_OK) {
@@ -342,18 +521,17 @@ int flush(p2g_ctx *ctx, Deferred *d)
             }
             q = q1;
         }
+        for (size_t q = g0; q < g1; ++q)
+            dix[work[q].dst] = -1;
         g0 = g1;
     }
     // the products have been enqueued: release their references
     std::vector<uint32_t> dead;
-    {
-        std::lock_guard<std::mutex> lock(d->pend_mu);
-        for (const Product &p : work) {
-            if (--d->mirrors[p.dst].refs == 0 && !d->mirrors[p.dst].current)
-                dead.push_back(p.dst);
-            if (--d->mirrors[p.src].refs == 0 && !d->mirrors[p.src].current)
-                dead.push_back(p.src);
-        }
+    for (const Product &p : work) {
+        if (--d->mirrors[p.dst].refs == 0 && !d->mirrors[p.dst].current)
+            dead.push_back(p.dst);
+        if (--d->mirrors[p.src].refs == 0 && !d->mirrors[p.src].current)
+            dead.push_back(p.src);
     }
     std::sort(dead.begin(), dead.end());
     dead.erase(std::unique(dead.begin(), dead.end()), dead.end());
@@ -364,7 +542,7 @@ int flush(p2g_ctx *ctx, Deferred *d)
 }
 
 // The current mirror of host address p covering at least `bytes`, or -1.
-// map_mu held (shared or exclusive).
+// A shard lock or the map write lock held.
 long find(Deferred *d, const void *p, size_t bytes)
 {
     auto it = d->by_host.find(reinterpret_cast<uintptr_t>(p));
@@ -373,21 +551,23 @@ long find(Deferred *d, const void *p, size_t bytes)
     return static_cast<long>(it->second);
 }
 
-// One recorded product.  pend_mu held, and map_mu (shared or exclusive).
-void add_product(Deferred *d, uint32_t dst, uint32_t src, size_t off, size_t len, uint16_t c)
+// One recorded product into shard `sh`.  sh.mu held (or the map write
+// lock); mirror reference counts and flags change atomically, as other
+// shards record products on the same mirrors.
+void add_product(Deferred *d, Shard &sh, uint32_t dst, uint32_t src, size_t off, size_t len,
+                 uint16_t c)
 {
     Mirror &md = d->mirrors[dst];
     Mirror &ms = d->mirrors[src];
-    if (ms.refs++ == 0 && !ms.dst)
-        d->pend_src_bytes += ms.bytes;
-    ++md.refs;
-    if (!md.dst) {
-        md.dst = true;
-        if (md.current)
-            ++d->live_dsts;
-    }
-    d->pending.push_back(Product{dst, src, off, len, c});
-    d->pend_macs += static_cast<double>(len);
+    if (__atomic_fetch_add(&ms.refs, 1, __ATOMIC_RELAXED) == 0 &&
+        !__atomic_load_n(&ms.dst, __ATOMIC_RELAXED))
+        sh.src_bytes += ms.bytes;
+    __atomic_fetch_add(&md.refs, 1, __ATOMIC_RELAXED);
+    if (!__atomic_load_n(&md.dst, __ATOMIC_RELAXED) &&
+        !__atomic_exchange_n(&md.dst, true, __ATOMIC_RELAXED) && md.current)
+        __atomic_fetch_add(&d->live_dsts, 1, __ATOMIC_RELAXED);
+    sh.pending.push_back(Product{dst, src, off, len, c});
+    sh.macs += static_cast<double>(len);
 }
 
 // Records dsts[o][off, off+len) ^= coeff(o, i) * srcs[i][off, off+len).
@@ -403,22 +583,34 @@ int record(p2g_ctx *ctx, uint16_t *const *dsts, size_t ndst, const uint16_t *con
         P2G_TRY(setup(ctx, d));
     }
     const size_t need = (off + len) * 2;
-    std::vector<long> dm(ndst), sm(nsrc);
-    bool all = true;
+    // mirror ids of the call's buffers (on the stack for small calls)
+    constexpr size_t kSmall = 16;
+    long dm_s[kSmall], sm_s[kSmall];
+    std::vector<long> dm_v, sm_v;
+    long *dm = dm_s, *sm = sm_s;
+    if (ndst > kSmall) {
+        dm_v.resize(ndst);
+        dm = dm_v.data();
+    }
+    if (nsrc > kSmall) {
+        sm_v.resize(nsrc);
+        sm = sm_v.data();
+    }
     {
-        std::shared_lock<std::shared_mutex> lock(d->map_mu);
-        for (size_t o = 0; o < ndst; ++o)
-            all = all && (dm[o] = find(d, dsts[o], need)) >= 0;
-        for (size_t i = 0; i < nsrc; ++i)
-            sm[i] = find(d, srcs[i], need);
-        const bool srcs_ok = std::all_of(sm.begin(), sm.end(), [](long v) { return v >= 0; });
-        if (all && srcs_ok) {
-            std::lock_guard<std::mutex> plock(d->pend_mu);
+        // every buffer prepared: record under this thread's shard lock
+        Shard &sh = my_shard(d);
+        std::lock_guard<std::mutex> lock(sh.mu);
+        bool all = true;
+        for (size_t o = 0; o < ndst && all; ++o)
+            all = (dm[o] = find(d, dsts[o], need)) >= 0;
+        for (size_t i = 0; i < nsrc && all; ++i)
+            all = (sm[i] = find(d, srcs[i], need)) >= 0;
+        if (all) {
             for (size_t o = 0; o < ndst; ++o)
                 for (size_t i = 0; i < nsrc; ++i) {
                     const uint16_t c = coeff(o, i);
                     if (c)
-                        add_product(d, static_cast<uint32_t>(dm[o]),
+                        add_product(d, sh, static_cast<uint32_t>(dm[o]),
                                     static_cast<uint32_t>(sm[i]), off, len, c);
                 }
             return P2G_OK;
@@ -427,7 +619,7 @@ int record(p2g_ctx *ctx, uint16_t *const *dsts, size_t ndst, const uint16_t *con
     // Some buffer is not prepared.
     std::unique_lock<std::mutex> lock(ctx->mu);
     P2G_CUDA(cudaSetDevice(ctx->device));
-    std::unique_lock<std::shared_mutex> wlock(d->map_mu);
+    MapWriteLock wlock(d);
     std::vector<size_t> prep, unprep;  // destinations with / without a mirror
     for (size_t o = 0; o < ndst; ++o) {
         dm[o] = find(d, dsts[o], need);
@@ -443,16 +635,13 @@ int record(p2g_ctx *ctx, uint16_t *const *dsts, size_t ndst, const uint16_t *con
             P2G_TRY(new_mirror(ctx, d, srcs[i], need, id));
             sm[i] = id;
         }
-        {
-            std::lock_guard<std::mutex> plock(d->pend_mu);
-            for (size_t o : prep)
-                for (size_t i = 0; i < nsrc; ++i) {
-                    const uint16_t c = coeff(o, i);
-                    if (c)
-                        add_product(d, static_cast<uint32_t>(dm[o]),
-                                    static_cast<uint32_t>(sm[i]), off, len, c);
-                }
-        }
+        for (size_t o : prep)
+            for (size_t i = 0; i < nsrc; ++i) {
+                const uint16_t c = coeff(o, i);
+                if (c)
+                    add_product(d, d->shard[0], static_cast<uint32_t>(dm[o]),
+                                static_cast<uint32_t>(sm[i]), off, len, c);
+            }
         // temporaries that ended up unused (all-zero coefficients) go now
         for (size_t i = 0; i < nsrc; ++i)
             if (!d->mirrors[sm[i]].current && d->mirrors[sm[i]].refs == 0 &&
@@ -500,9 +689,16 @@ void deferred_release(p2g_ctx *ctx)
         return;
     cudaStreamSynchronize(ctx->stream);
     cudaStreamSynchronize(ctx->copy_stream);
+    delete d->copier;
     for (Mirror &m : d->mirrors)
         if (m.dev)
             cudaFree(m.dev);
+    for (FreeBlock &b : d->free_blocks) {
+        cudaFree(b.dev);
+        cudaEventDestroy(b.ev);
+    }
+    for (cudaEvent_t ev : d->spare_events)
+        cudaEventDestroy(ev);
     if (d->pool)
         cudaMemPoolDestroy(d->pool);
     for (int i = 0; i < kStageChunks; ++i) {
@@ -545,13 +741,15 @@ int p2g_prepare_shuffle2x(p2g_ctx *ctx, uint16_t *data, size_t n)
     P2G_CUDA(cudaSetDevice(ctx->device));
     Deferred *d = nullptr;
     P2G_TRY(setup(ctx, d));
-    std::unique_lock<std::shared_mutex> wlock(d->map_mu);
+    MapWriteLock wlock(d);
     // between the caller's batches: run what has accumulated
-    bool due;
-    {
-        std::lock_guard<std::mutex> plock(d->pend_mu);
-        due = d->pend_macs >= kFlushMacs || d->pend_src_bytes >= kFlushSourceBytes;
+    double macs = 0;
+    size_t src_bytes = 0;
+    for (const Shard &sh : d->shard) {
+        macs += sh.macs;
+        src_bytes += sh.src_bytes;
     }
+    const bool due = macs >= kFlushMacs || src_bytes >= kFlushSourceBytes;
     if (due)
         P2G_TRY(flush(ctx, d));
     const long old = find(d, data, 0);
@@ -612,7 +810,7 @@ int p2g_finish_shuffle2x(p2g_ctx *ctx, uint16_t *data, size_t n)
     P2G_CUDA(cudaSetDevice(ctx->device));
     Deferred *d = nullptr;
     P2G_TRY(setup(ctx, d));
-    std::unique_lock<std::shared_mutex> wlock(d->map_mu);
+    MapWriteLock wlock(d);
     const long id = find(d, data, 0);
     if (id < 0)
         return P2G_OK;  // never prepared: the buffer already holds its data

@@ -220,10 +220,15 @@ class StreamingEncoder {
         for (size_t e = 0; e < r_; ++e) {
             out[e].first = static_cast<uint32_t>(e);
             out[e].second.resize(bs_ - bs_ % 2);
+#if defined(__BYTE_ORDER__) && __BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__
+            // the symbols' little-endian bytes are their memory image here
+            memcpy(out[e].second.data(), recovery_[e].data(), spb_ * 2);
+#else
             for (size_t x = 0; x < spb_; ++x) {
                 out[e].second[2 * x] = static_cast<uint8_t>(recovery_[e][x]);
                 out[e].second[2 * x + 1] = static_cast<uint8_t>(recovery_[e][x] >> 8);
             }
+#endif
         }
         return out;
     }
