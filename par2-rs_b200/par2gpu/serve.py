@@ -3,7 +3,8 @@
 Two servers over the same arrival stream:
 
 * ``serve_continuous`` -- continuous batching.  Arrived jobs are admitted in
-  arrival order while their scratch fits an HBM budget; every admitted job is
+  arrival order while their scratch fits an HBM budget and the device's free
+  memory (a job is always admitted when nothing else runs); every admitted job is
   cut into work units (column ranges of create / repair jobs, slice groups of
   verify jobs, each bounded in work); each iteration takes units round-robin
   from all admitted jobs up to an iteration work budget and runs them as one
@@ -68,6 +69,16 @@ class ServedJob:
         records = self.k * self.n * (96 if self.n <= 24 else 32)
         rhs = self.n * self.S if self.kind == "repair" else 0
         return self.n * self.S + planes + records + rhs
+
+
+def _fits_device(job, margin=1 << 30):
+    """Whether the device holds the job's scratch now, beside what the
+    running jobs and everything else on it already use (the budget counts
+    estimates; this counts real free memory, with a margin)."""
+    import torch
+
+    free, _ = torch.cuda.mem_get_info(job.src.device)
+    return job.scratch_bytes() + margin <= free
 
 
 def _alloc_outputs(job):
@@ -194,7 +205,8 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
         while nxt < n and arrivals[order[nxt]] <= t:
             queue.append(jobs[order[nxt]])
             nxt += 1
-        while queue and used + queue[0].scratch_bytes() <= budget_bytes:
+        while queue and used + queue[0].scratch_bytes() <= budget_bytes and \
+                (not active or _fits_device(queue[0])):
             job = queue.popleft()
             used += job.scratch_bytes()
             _alloc_outputs(job)
