@@ -71,14 +71,25 @@ class ServedJob:
         return self.n * self.S + planes + records + rhs
 
 
-def _fits_device(job, margin=1 << 30):
-    """Whether the device holds the job's scratch now, beside what the
-    running jobs and everything else on it already use (the budget counts
-    estimates; this counts real free memory, with a margin)."""
-    import torch
+class _DeviceRoom:
+    """Real free device memory for admission (the budget counts estimates):
+    read at most every `every` seconds, less the scratch of the jobs
+    admitted since the reading."""
 
-    free, _ = torch.cuda.mem_get_info(job.src.device)
-    return job.scratch_bytes() + margin <= free
+    def __init__(self, every=0.05, margin=1 << 30):
+        self.every, self.margin = every, margin
+        self.free, self.t, self.since = None, -1.0, 0
+
+    def fits(self, job, t):
+        import torch
+
+        if self.free is None or t - self.t > self.every:
+            self.free = torch.cuda.mem_get_info(job.src.device)[0]
+            self.t, self.since = t, 0
+        return job.scratch_bytes() + self.margin <= self.free - self.since
+
+    def admitted(self, job):
+        self.since += job.scratch_bytes()
 
 
 def _alloc_outputs(job):
@@ -157,6 +168,7 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
     done = 0
     inflight = None                    # (batch, [(jid, unit)...], ctx index)
     prepared = None
+    room = _DeviceRoom()
     ci = 0
     t0 = time.perf_counter()
 
@@ -206,9 +218,10 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
             queue.append(jobs[order[nxt]])
             nxt += 1
         while queue and used + queue[0].scratch_bytes() <= budget_bytes and \
-                (not active or _fits_device(queue[0])):
+                (not active or room.fits(queue[0], t)):
             job = queue.popleft()
             used += job.scratch_bytes()
+            room.admitted(job)
             _alloc_outputs(job)
             if job.kind == "repair":
                 job.inverse = aux.reconstruction_matrix(job.k, job.missing, np.arange(job.m))
