@@ -805,6 +805,43 @@ def run_batched(args):
     print(json.dumps(batched_leg()), flush=True)
 
 
+def run_profile_batched(args):
+    """An ncu-sized batch for the persistent kernel: the first 48 create sets
+    of the batched distribution whose sources are at most 64 MiB, in one
+    batch (one persistent launch), run `--warmup` + `--steps` times."""
+    import torch
+
+    import par2gpu
+
+    dev = torch.device("cuda", 0)
+    sets = [x for x in batched_sets(SEED + 7, 1024) if x["create"] and x["k"] * x["S"] <= 64 << 20][:48]
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 9)
+    ctx = par2gpu.Context(0)
+    jobs, keep = [], []
+    for x in sets:
+        src = torch.randint(0, 256, (x["k"], x["S"]), dtype=torch.uint8, device=dev, generator=g)
+        out = torch.zeros((x["r"], x["S"]), dtype=torch.uint8, device=dev)
+        keep += [src, out]
+        jobs.append({"kind": par2gpu.JOB_CREATE, "k": x["k"], "slice_bytes": x["S"], "src": src,
+                     "exps": np.arange(x["r"]), "out": out})
+    ms = []
+    for step in range(args.warmup + max(1, args.steps)):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        b = par2gpu.Batch(ctx, jobs)
+        st = b.run()
+        b.close()
+        ms.append((time.perf_counter() - t0) * 1e3)
+        assert all(v == 0 for v in st), st
+    macs = sum(x["k"] * x["r"] * (x["S"] // 2) for x in sets)
+    print(json.dumps({"workload": "profile_batched: 48 create sets of the batched distribution, "
+                                  "sources at most 64 MiB each, one batch",
+                      "sets": len(sets), "source_bytes": sum(x["k"] * x["S"] for x in sets),
+                      "symbol_macs": macs, "ms_per_run": ms[args.warmup:]}), flush=True)
+    ctx.close()
+
+
 def batched_leg():
     """Many independent sets: per-set plain calls (p2g_encode / p2g_repair,
     one set after another) against the batch executor (one persistent kernel
@@ -1110,7 +1147,7 @@ def main():
     ap.add_argument("--workload", default="large_encode",
                     choices=sorted(WORKLOADS) + sorted(HASH_WORKLOADS) +
                     ["verify_repair", "invert", "create_files", "batched",
-                     "serving"])
+                     "serving", "profile_batched"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the heuristic tile shape instead of the autotuned one")
     ap.add_argument("--quick", action="store_true",
@@ -1133,6 +1170,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args)
+        return
+    if args.workload == "profile_batched":
+        run_profile_batched(args)
         return
     if args.workload == "serving":
         run_serving(args)
