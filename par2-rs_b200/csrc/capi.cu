@@ -588,6 +588,15 @@ int p2g_encode(p2g_ctx *ctx, const uint8_t *const *src, size_t k, size_t slice_b
     std::vector<size_t> cut(slabs + 1);
     for (int q = 0; q <= slabs; ++q)
         cut[q] = q == slabs ? slice_bytes : tiles * q / slabs * 2048;
+    // The last slab's compute and read-back are what remains after the last
+    // upload: it goes in two halves, the first computed and read back while
+    // the second uploads.
+    if (tail && slabs < kMaxTailSlabs) {
+        const size_t a = cut[slabs - 1] / 2048, b = tiles;
+        if (b - a >= 2)
+            cut.insert(cut.end() - 1, (a + (b - a) / 2) * 2048);
+    }
+    slabs = static_cast<int>(cut.size()) - 1;
     const size_t tail_bytes = tail ? slabs * (ntail + r) * sizeof(void *) : 0;
     ParamLayout L(k, r, k * 2, round16(r * 4) + tail_bytes);
     P2G_TRY(ctx->hparams.ensure(L.total));
