@@ -863,10 +863,24 @@ int p2g_reconstruction_matrix(p2g_ctx *ctx, size_t k, const uint64_t *missing, s
     return finish(ctx);
 }
 
+// Column slabs of a host-buffer repair's last input groups: each slab's
+// present columns go up, both passes run on the slab, and its finished
+// output columns go back while the next slab uploads.
+struct RepairTail {
+    int slabs = 0;             // 0: no slabs
+    int groups = 0;            // upload groups in the tail
+    size_t t0 = 0, ntail = 0;  // the tail's present slices [t0, t0 + ntail)
+    std::vector<size_t> cut;   // slab q: columns [cut[q], cut[q + 1])
+    size_t tab_off = 0;        // per slab: ntail inputs, m RHS, m outputs (device pointers)
+    const uint8_t *const *present = nullptr;  // the caller's host slices
+    const std::vector<uint8_t *> *ps = nullptr;  // their device copies
+};
+
 static int repair_passes(p2g_ctx *ctx, size_t m, size_t np, size_t slice_bytes, int groups,
                          uint8_t *dp, const ParamLayout &L, size_t exps_off,
                          const uint32_t *exps, uint8_t *const *out,
-                         const std::vector<uint8_t *> &os, bool o_st, bool dev);
+                         const std::vector<uint8_t *> &os, bool o_st, bool dev,
+                         const RepairTail &tail);
 
 int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missing, size_t m,
                const uint8_t *const *present, const uint32_t *exps,
@@ -923,8 +937,40 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
     P2G_TRY(copy_slices(rhs.data(), recovery, m, slice_bytes,
                         dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     P2G_TRY(stage(ctx, ctx->out_copy, out, m, slice_bytes, dev, false, os, o_st));
-    // parameter block: [present ptrs][rhs ptrs | out ptrs][cmiss | exps | cpres]
-    ParamLayout L(np, 2 * m, m * 2 + m * 4 + 16, np * 2);
+    // With host outputs, the last groups of present slices run slab by slab
+    // (as in p2g_encode): what remains after the last upload is one slab's
+    // passes and read-back instead of the whole second pass and the
+    // read-back of every output.  Slabs about fill the device each.
+    RepairTail tail;
+    const size_t tiles = (slice_bytes + 2047) / 2048;
+    if (groups >= 4 && o_st) {
+        // the last kTailGroups groups (measured on 2048 x 1 MiB, m = 205:
+        // 45.1 ms with 2, 46.7 with 4, 47.7 with 6; 48.8 without slabs)
+        const int tg = std::min(kTailGroups, groups - 1);
+        const p2g::MuladdPlan tp = p2g::choose_plan(
+            ctx, static_cast<int>(np / groups * tg), static_cast<int>(m), slice_bytes);
+        const double waves = static_cast<double>(p2g::plan_tiles(tp, slice_bytes)) * tp.nblk /
+                             p2g::plan_slots(ctx, tp);
+        int slabs = static_cast<int>(std::min<double>(kMaxTailSlabs - 1, std::floor(waves + 0.5)));
+        if (slabs >= 2 && static_cast<size_t>(slabs) <= tiles) {
+            for (int q = 0; q <= slabs; ++q)
+                tail.cut.push_back(q == slabs ? slice_bytes : tiles * q / slabs * 2048);
+            // the last slab in two halves (see p2g_encode)
+            const size_t a = tail.cut[slabs - 1] / 2048;
+            if (tiles - a >= 2)
+                tail.cut.insert(tail.cut.end() - 1, (a + (tiles - a) / 2) * 2048);
+            tail.slabs = static_cast<int>(tail.cut.size()) - 1;
+            tail.groups = tg;
+            tail.t0 = np * (groups - tg) / groups;
+            tail.ntail = np - tail.t0;
+            tail.present = present;
+            tail.ps = &ps;
+        }
+    }
+    const size_t tail_bytes =
+        tail.slabs ? tail.slabs * (tail.ntail + 2 * m) * sizeof(void *) : 0;
+    // parameter block: [present ptrs][rhs ptrs | out ptrs][cmiss | exps | cpres | slab tables]
+    ParamLayout L(np, 2 * m, m * 2 + m * 4 + 16, round16(np * 2) + tail_bytes);
     P2G_TRY(ctx->hparams.ensure(L.total));
     P2G_TRY(ctx->params.ensure(L.total));
     uint8_t *h = ctx->hparams.as<uint8_t>();
@@ -936,14 +982,27 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
     memcpy(h + exps_off, exps, m * 4);
     if (np)
         memcpy(h + L.b_off, cpres.data(), np * 2);
+    if (tail.slabs) {
+        tail.tab_off = L.b_off + round16(np * 2);
+        uint8_t **t = reinterpret_cast<uint8_t **>(h + tail.tab_off);
+        for (int q = 0; q < tail.slabs; ++q) {
+            for (size_t i = 0; i < tail.ntail; ++i)
+                *t++ = ps[tail.t0 + i] + tail.cut[q];
+            for (size_t j = 0; j < m; ++j)
+                *t++ = rhs[j] + tail.cut[q];
+            for (size_t j = 0; j < m; ++j)
+                *t++ = os[j] + tail.cut[q];
+        }
+    }
     P2G_TRY(upload_params(ctx, L));
     uint8_t *dp = ctx->params.as<uint8_t>();
     if (groups > 1) {
         // after everything already queued on the compute stream (earlier
-        // users of the staging buffers)
+        // users of the staging buffers); the tail groups go up slab by slab
+        // in repair_passes
         P2G_CUDA(cudaEventRecord(ctx->pipe_ev[0], ctx->stream));
         P2G_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ev[0], 0));
-        for (int g = 0; g < groups; ++g) {
+        for (int g = 0; g < (tail.slabs ? groups - tail.groups : groups); ++g) {
             const size_t i0 = np * g / groups, i1 = np * (g + 1) / groups;
             const int rc = copy_slices(ps.data() + i0, present + i0, i1 - i0, slice_bytes,
                                        cudaMemcpyHostToDevice, ctx->copy_stream);
@@ -958,9 +1017,12 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
     // every return below waits for the uploads still reading the caller's
     // present slices
     const int rc = repair_passes(ctx, m, np, slice_bytes, groups, dp, L, exps_off, exps, out, os,
-                                 o_st, dev);
-    if (groups > 1)
+                                 o_st, dev, tail);
+    if (groups > 1) {
         cudaStreamSynchronize(ctx->copy_stream);
+        if (tail.slabs)
+            cudaStreamSynchronize(ctx->d2h_stream);
+    }
     return rc;
 }
 
@@ -968,7 +1030,8 @@ int p2g_repair(p2g_ctx *ctx, size_t k, size_t slice_bytes, const uint64_t *missi
 static int repair_passes(p2g_ctx *ctx, size_t m, size_t np, size_t slice_bytes, int groups,
                          uint8_t *dp, const ParamLayout &L, size_t exps_off,
                          const uint32_t *exps, uint8_t *const *out,
-                         const std::vector<uint8_t *> &os, bool o_st, bool dev)
+                         const std::vector<uint8_t *> &os, bool o_st, bool dev,
+                         const RepairTail &tail)
 {
     const uint32_t *d_exps = reinterpret_cast<const uint32_t *>(dp + exps_off);
     // 1. A^-1 on the device
@@ -989,7 +1052,8 @@ static int repair_passes(p2g_ctx *ctx, size_t m, size_t np, size_t slice_bytes, 
                              static_cast<int>(np), static_cast<int>(m), ctx->recs.as<uint32_t>()));
         const uint8_t *const *d_src = reinterpret_cast<const uint8_t *const *>(dp + L.src_off);
         const size_t rw = static_cast<size_t>(record_words(static_cast<int>(m)));
-        for (int g = 0; g < groups; ++g) {
+        const int full = tail.slabs ? groups - tail.groups : groups;
+        for (int g = 0; g < full; ++g) {
             const size_t i0 = np * g / groups, i1 = np * (g + 1) / groups;
             if (groups > 1)
                 P2G_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[g], 0));
@@ -1003,12 +1067,53 @@ static int repair_passes(p2g_ctx *ctx, size_t m, size_t np, size_t slice_bytes, 
     P2G_TRY(ctx->recs2.ensure(record_bytes(m, static_cast<int>(m))));
     P2G_TRY(records_from_matrix(ctx, ctx->inv.as<uint16_t>(), static_cast<int>(m),
                                 static_cast<int>(m), ctx->recs2.as<uint32_t>()));
-    P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.dst_off),
-                       static_cast<int>(m),
-                       reinterpret_cast<uint8_t *const *>(dp + L.dst_off + m * sizeof(void *)),
-                       static_cast<int>(m), slice_bytes, ctx->recs2.as<uint32_t>(), 0));
-    if (o_st)
-        P2G_TRY(unstage(ctx, out, os, m, slice_bytes, dev));
+    if (!tail.slabs) {
+        P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(dp + L.dst_off),
+                           static_cast<int>(m),
+                           reinterpret_cast<uint8_t *const *>(dp + L.dst_off + m * sizeof(void *)),
+                           static_cast<int>(m), slice_bytes, ctx->recs2.as<uint32_t>(), 0));
+        if (o_st)
+            P2G_TRY(unstage(ctx, out, os, m, slice_bytes, dev));
+        return finish(ctx);
+    }
+    // Tail slabs: the slab's present columns go up, step 2 finishes the
+    // slab's right-hand sides, step 3 forms its missing columns, which go
+    // back on the read-back stream while the next slab uploads.  (A failed
+    // step returns after the copies already enqueued, see p2g_repair.)
+    const size_t rw = static_cast<size_t>(record_words(static_cast<int>(m)));
+    uint8_t *const *tab = reinterpret_cast<uint8_t *const *>(dp + tail.tab_off);
+    const size_t per = tail.ntail + 2 * m;
+    std::vector<const uint8_t *> hs(tail.ntail);
+    std::vector<uint8_t *> ds(tail.ntail), uo(m), so(m);
+    cudaEvent_t *up = ctx->pipe_ev + kSlabEvents, *done = up + tail.slabs;
+    for (int q = 0; q < tail.slabs; ++q) {
+        const size_t c0 = tail.cut[q], w = tail.cut[q + 1] - c0;
+        for (size_t i = 0; i < tail.ntail; ++i) {
+            hs[i] = tail.present[tail.t0 + i] + c0;
+            ds[i] = (*tail.ps)[tail.t0 + i] + c0;
+        }
+        P2G_TRY(copy_slices(ds.data(), hs.data(), tail.ntail, w, cudaMemcpyHostToDevice,
+                            ctx->copy_stream));
+        P2G_CUDA(cudaEventRecord(up[q], ctx->copy_stream));
+        P2G_CUDA(cudaStreamWaitEvent(ctx->stream, up[q], 0));
+        uint8_t *const *qt = tab + q * per;
+        P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(qt),
+                           static_cast<int>(tail.ntail), qt + tail.ntail, static_cast<int>(m), w,
+                           ctx->recs.as<uint32_t>() + tail.t0 * m * rw, 1));
+        P2G_TRY(muladd_run(ctx, reinterpret_cast<const uint8_t *const *>(qt + tail.ntail),
+                           static_cast<int>(m), qt + tail.ntail + m, static_cast<int>(m), w,
+                           ctx->recs2.as<uint32_t>(), 0));
+        P2G_CUDA(cudaEventRecord(done[q], ctx->stream));
+        P2G_CUDA(cudaStreamWaitEvent(ctx->d2h_stream, done[q], 0));
+        for (size_t j = 0; j < m; ++j) {
+            uo[j] = out[j] + c0;
+            so[j] = os[j] + c0;
+        }
+        P2G_TRY(copy_slices(uo.data(), so.data(), m, w, cudaMemcpyDeviceToHost, ctx->d2h_stream));
+    }
+    // the call ends when the last read-back has landed
+    P2G_CUDA(cudaEventRecord(done[tail.slabs], ctx->d2h_stream));
+    P2G_CUDA(cudaStreamWaitEvent(ctx->stream, done[tail.slabs], 0));
     return finish(ctx);
 }
 

@@ -198,6 +198,24 @@ def test_repair_from_host_buffers_in_upload_groups(ctx, m):
     assert np.array_equal(got, want) and np.array_equal(got, src[missing])
 
 
+@pytest.mark.parametrize("m", [13, 205])
+def test_repair_from_host_buffers_with_slab_tail(ctx, m):
+    """Wide host slices (1 MiB + 2 bytes): the last two upload groups run as
+    column slabs -- each slab's present columns go up, both passes run on
+    it, its rebuilt columns come back while the next slab uploads.  The
+    rebuilt slices equal the erased ones (small-output and paired records)."""
+    rng = np.random.default_rng(91 + m)
+    k, S = 600, (1 << 20) + 2
+    src = rng.integers(0, 256, (k, S), dtype=np.uint8)
+    exps = np.arange(m, dtype=np.uint32)
+    rec = ctx.encode_array(src, exps)
+    missing = np.sort(rng.choice(k, m, replace=False))
+    data = src.copy()
+    data[missing] = 0
+    got = ctx.repair_array(data, missing, exps, rec)
+    assert np.array_equal(got, src[missing])
+
+
 def test_singular_repair_while_uploads_are_in_flight(ctx):
     """Beyond 32768 slices the constants repeat, so losing slices 5 and
     5 + 32768 leaves a singular matrix: the host-buffer repair (present slices
