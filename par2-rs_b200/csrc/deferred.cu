@@ -331,8 +331,10 @@ int take_block(p2g_ctx *ctx, Deferred *d, size_t bytes, uint8_t *&dev)
             continue;
         const cudaError_t q = cudaEventQuery(b.ev);
         if (q == cudaErrorNotReady) {
+            // blocks are kept oldest first and their events complete in
+            // stream order: no younger block is free yet either
             (void)cudaGetLastError();
-            continue;
+            break;
         }
         P2G_CUDA(q);
         dev = b.dev;
