@@ -73,10 +73,11 @@ class ServedJob:
 
 class _DeviceRoom:
     """Real free device memory for admission (the budget counts estimates):
-    read at most every `every` seconds, less the scratch of the jobs
+    the driver's free memory plus what torch's caching allocator holds
+    unused, read at most every `every` seconds, less the scratch of the jobs
     admitted since the reading."""
 
-    def __init__(self, every=0.05, margin=1 << 30):
+    def __init__(self, every=0.05, margin=256 << 20):
         self.every, self.margin = every, margin
         self.free, self.t, self.since = None, -1.0, 0
 
@@ -84,7 +85,9 @@ class _DeviceRoom:
         import torch
 
         if self.free is None or t - self.t > self.every:
-            self.free = torch.cuda.mem_get_info(job.src.device)[0]
+            dev = job.src.device
+            cached = torch.cuda.memory_reserved(dev) - torch.cuda.memory_allocated(dev)
+            self.free = torch.cuda.mem_get_info(dev)[0] + cached
             self.t, self.since = t, 0
         return job.scratch_bytes() + self.margin <= self.free - self.since
 

@@ -40,6 +40,8 @@ def test_device_room_reads_free_memory_sparingly(monkeypatch):
         return (3 << 30, 180 << 30)
 
     monkeypatch.setattr(torch.cuda, "mem_get_info", fake_mem_get_info)
+    monkeypatch.setattr(torch.cuda, "memory_reserved", lambda device=None: 0)
+    monkeypatch.setattr(torch.cuda, "memory_allocated", lambda device=None: 0)
     room = _DeviceRoom(every=0.05, margin=1 << 30)
     job = ServedJob(0, "create", np.zeros((2048, 1 << 20), np.uint8), r=1)  # 2 GiB of planes + 2 MB
     small = ServedJob(1, "create", np.zeros((64, 1 << 20), np.uint8), r=8)  # ~72 MiB
