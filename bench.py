@@ -1156,7 +1156,7 @@ def serving_leg(rates):
     results = []
     for lam in rates:
         rng = np.random.default_rng(SEED + lam)
-        nj = int(min(240, max(120, lam * 1.5)))
+        nj = int(min(600, max(120, lam * 2)))  # p99 of 120-600 jobs
         arrivals = np.cumsum(rng.exponential(1.0 / lam, nj))
         jobs_a = make_jobs(pool, nj, np.random.default_rng(SEED + 100 + lam), ctxs[0])
         jobs_b = make_jobs(pool, nj, np.random.default_rng(SEED + 100 + lam), ctxs[0])
