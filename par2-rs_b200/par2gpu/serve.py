@@ -164,7 +164,7 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
     order = np.argsort(arrivals, kind="stable")
     lat = np.zeros(n)
     queue = collections.deque()
-    active = collections.deque()       # [job, pending units deque, outstanding count]
+    active = collections.deque()       # [job, pending units deque, outstanding count, admission no.]
     state = {}
     used = 0
     nxt = 0
@@ -172,6 +172,7 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
     inflight = None                    # (batch, [(jid, unit)...], ctx index)
     prepared = None
     room = _DeviceRoom()
+    admitted = 0
     ci = 0
     t0 = time.perf_counter()
 
@@ -187,6 +188,14 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
         picked, work = [], 0.0
         alone = sum(1 for e in active if e[1]) == 1 and not queue
         budget = iter_macs * (16 if alone else 1)
+        # the oldest job with work left takes up to half the budget first
+        # (the longest-running jobs make the latency tail), then every job
+        # takes units in turn
+        oldest = min((e for e in active if e[1]), key=lambda e: e[3], default=None)
+        while oldest is not None and oldest[1] and work < budget / 2:
+            u = oldest[1].popleft()
+            picked.append((oldest[0], u))
+            work += _unit_work(oldest[0], u)
         progress = True
         while progress and work < budget:
             progress = False
@@ -229,7 +238,8 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
             if job.kind == "repair":
                 job.inverse = aux.reconstruction_matrix(job.k, job.missing, np.arange(job.m))
             units = collections.deque(_units(job, unit_macs))
-            ent = [job, units, len(units)]
+            ent = [job, units, len(units), admitted]
+            admitted += 1
             state[job.jid] = ent
             active.append(ent)
         if inflight is not None and inflight[0].poll():
