@@ -6,8 +6,9 @@ Two servers over the same arrival stream:
   arrival order while their scratch fits an HBM budget and the device's free
   memory (a job is always admitted when nothing else runs); every admitted job is
   cut into work units (column ranges of create / repair jobs, slice groups of
-  verify jobs, each bounded in work); each iteration takes units round-robin
-  from all admitted jobs up to an iteration work budget and runs them as one
+  verify jobs, each bounded in work); each iteration gives the oldest admitted
+  job up to half of an iteration work budget, fills the rest with units taken
+  round-robin from all admitted jobs and runs them as one
   batch (``Batch``: one persistent kernel per phase).  The next batch is
   prepared on a second context while the current one runs, so jobs that
   arrive while others are on the GPU join at the next iteration and their
@@ -180,8 +181,9 @@ def serve_continuous(ctxs, jobs, arrivals, budget_bytes=120 << 30, iter_macs=4e1
         return time.perf_counter() - t0
 
     def build(ctx):
-        """Pick units round-robin from admitted jobs up to the iteration
-        budget, then merge each job's contiguous units into one spec so that
+        """Pick units up to the iteration budget -- the oldest job with work
+        left first, up to half of it, then round-robin from all admitted
+        jobs -- and merge each job's contiguous units into one spec so that
         its coefficient records are built once per batch.  A job alone with
         nothing queued gets 16 budgets: cutting it finer only rebuilds its
         records, and a job that arrives meanwhile waits for at most that."""
