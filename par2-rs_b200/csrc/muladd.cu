@@ -434,9 +434,9 @@ __device__ __forceinline__ void muladd_item(uint8_t *smem, const uint32_t *__res
         __syncthreads();
         for (int i = i0; i < i1; ++i) {
             issue(i + 3);
+            consume(i, (i - i0) & 1);
             if (i + 1 < i1)
                 build(i + 1, (i + 1 - i0) & 1);
-            consume(i, (i - i0) & 1);
             cp_async_wait<1>();
             __syncthreads();
         }
@@ -666,7 +666,8 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
     };
 
     if constexpr (STAGE == 1) {
-        // one input per barrier: build input i + 1 while consuming input i
+        // one input per barrier: consume input i, then build input i + 1
+        // (lookups first: 2 % faster than building first)
         if (i0 < i1) {
             issue(i0);
             issue(i0 + 1);
@@ -677,18 +678,19 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
             __syncthreads();
             for (int i = i0; i < i1; ++i) {
                 issue(i + 3);
+                consume(i, (i - i0) & 1);
                 if (i + 1 < i1)
                     build(i + 1, (i + 1 - i0) & 1);
-                consume(i, (i - i0) & 1);
                 cp_async_wait<1>();
                 __syncthreads();
             }
         }
     } else {
         // two inputs per barrier (four table buffers, eight ring slots):
-        // stage s consumes inputs s, s + 1 from one table pair, builds s + 2,
-        // s + 3 into the other and fetches s + 6, s + 7, whose copies may
-        // still be in flight at the barrier that ends the stage (s + 4, s + 5,
+        // stage s consumes inputs s, s + 1 from one table pair, then builds
+        // s + 2, s + 3 into the other (lookups first: 1 % faster than
+        // building first), and fetches s + 6, s + 7, whose copies may still
+        // be in flight at the barrier that ends the stage (s + 4, s + 5,
         // fetched a stage earlier, must have landed by then)
         if (i0 < i1) {
 #pragma unroll
@@ -705,13 +707,13 @@ __device__ __forceinline__ void muladd_item_paired(uint8_t *smem, const uint32_t
                 const int tp = ((s - i0) >> 1) & 1;
                 issue(s + 6);
                 issue(s + 7);
+                consume(s, 2 * tp);
+                if (s + 1 < i1)
+                    consume(s + 1, 2 * tp + 1);
                 if (s + 2 < i1)
                     build(s + 2, 2 * (tp ^ 1));
                 if (s + 3 < i1)
                     build(s + 3, 2 * (tp ^ 1) + 1);
-                consume(s, 2 * tp);
-                if (s + 1 < i1)
-                    consume(s + 1, 2 * tp + 1);
                 cp_async_wait<2>();
                 __syncthreads();
             }
