@@ -119,10 +119,10 @@ class CopyPool {
         for (std::thread &t : th_)
             t.join();
     }
-    // n bytes from src to dst in up to helpers + 1 parts of at least 256 KiB
+    // n bytes from src to dst in up to helpers + 1 parts of at least 128 KiB
     void copy(uint8_t *dst, const uint8_t *src, size_t n)
     {
-        const size_t parts = std::min<size_t>(th_.size() + 1, std::max<size_t>(1, n >> 18));
+        const size_t parts = std::min<size_t>(th_.size() + 1, std::max<size_t>(1, n >> 17));
         if (parts <= 1) {
             memcpy(dst, src, n);
             return;
@@ -269,10 +269,10 @@ int setup(p2g_ctx *ctx, Deferred *&out)
         }
     }
     if (rc == P2G_OK) {
-        // helpers for the staging copies: up to 3 more threads, leaving the
-        // host's other cores to the caller's workers
+        // helpers for the staging copies: up to 7 more threads (the callers
+        // prepare between their batches, when their workers are idle)
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        d->copier = new CopyPool(static_cast<int>(std::min(3u, hw / 4)));
+        d->copier = new CopyPool(static_cast<int>(std::min(7u, hw / 2)));
     }
     if (rc != P2G_OK) {
         (void)cudaGetLastError();

@@ -125,7 +125,7 @@ def test_streaming_encoder_quickpar():
 
 @pytest.mark.parametrize("k,S,r,threads", [(1, 64, 1, 1), (37, 4098, 13, 3), (300, 8192, 60, 8),
                                            (129, 65536, 205, 16),
-                                           # ragged blocks above 512 KiB: staging copies in parts
+                                           # ragged blocks above 256 KiB: staging copies in parts
                                            (64, (1 << 20) + 6, 9, 8)])
 def test_streaming_encoder_matches_oracle(k, S, r, threads):
     from par2gpu import format as fmt
