@@ -300,9 +300,10 @@ int p2g_batch_destroy(p2g_batch *batch);
  * problem of that class (8, 64, 160 or 420 outputs of ten times as many
  * inputs; slices of 8 KiB or 256 KiB; up to 64 copies of a small problem in
  * one launch, as many as make about 2e9 symbol multiply-accumulates; best
- * of `reps` launches of the persistent kernel after a warm-up) and keeps the
- * fastest per class
- * for this context's later batches.  forms_out / ms_out (optional,
+ * of `reps` launches of the persistent kernel after a warm-up) and keeps per
+ * class, for this context's later batches, the default form (small tables up
+ * to 24 outputs, paired above 104, wide between) unless another is at least
+ * 3 % faster.  forms_out / ms_out (optional,
  * P2G_BATCH_CLASSES entries) receive the chosen forms and their times. */
 int p2g_batch_autotune(p2g_ctx *ctx, int reps, int *forms_out, float *ms_out);
 /* Pins the form per class (P2G_BATCH_CLASSES entries; -1, or forms NULL,
